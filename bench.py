@@ -1,0 +1,379 @@
+"""Benchmark of the PDLP hot path on one node.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Workload: the synthetic LP with known optimum at scale -- m = 2,000,000
+equality rows, n = 5,000,000 columns, 8 nonzeros per column (40M nonzeros,
+FP64 values, int32 indices), Ruiz scaling with 10 passes -- solved to 1e-8
+relative KKT (the reference's definition).  One step = one full PDLP solve
+(setup, Ruiz, transpose, every iteration and restart check) of that LP.
+
+* ``value``: PDHG iterations per second over the timed solves, inputs
+  resident in HBM (device arrays handed to the C ABI), whole job (sum over
+  ranks / max time over ranks).
+* ``e2e``: the same through the public API with pinned HOST buffers; the
+  host->device copy of the model and the device->host copy of the solution
+  are inside the timed region.
+* ``roofline``: the dominant kernel's algorithmic bytes per launch over its
+  mean CUDA-event duration (profiled solve, launching stream), against the
+  measured HBM copy bandwidth.
+* ``cpu_baseline``: the reference's own CPU solve_pdlp (oracle/_ref, built
+  from the reference sources) on the same LP, rank 0, one core: setup-only
+  and 40-iteration samples, steady iterations/s.
+* ``--impl reference``: the reference CPU PDLP alone, same metric and config.
+
+N > 1 (torchrun): a single LP does not shard (replicas only), so every rank
+solves its own replica; no collective touches the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "markov-zip1_b200"))
+sys.path.insert(0, str(ROOT / "oracle"))
+
+METRIC = "time-to-1e-8 KKT & SpMV HBM GB/s: plain FP64 vs FP32+refine+warm-start PDLP"
+UNIT = "PDHG iterations/s (solve to 1e-8 relative KKT)"
+WORKLOAD = dict(m=2_000_000, n=5_000_000, k=8, seed=1)
+TOL = 1e-8
+
+
+def peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def kernel_bytes(kind: str, m: int, n: int, nnz: int, fp: int = 8) -> float:
+    """Algorithmic bytes of one launch of a fused kernel (each array touched once).
+
+    primal: col pointers 4(n+1), row indices 4nnz, values fp*nnz, the y gather
+            fp*m, reads c, col_norm, lo, hi, x, x_avg (6 fp n), writes x,
+            x_bar, x_avg (3 fp n)
+    dual:   row pointers 4(m+1), column indices 4nnz, values fp*nnz, the x_bar
+            gather fp*n, reads y, y_avg, b_lo, b_hi, row_norm (5 fp m),
+            writes y, y_avg (2 fp m)
+    """
+    if kind == "primal":
+        return 4 * (n + 1) + (4 + fp) * nnz + fp * m + 9 * fp * n
+    if kind == "dual":
+        return 4 * (m + 1) + (4 + fp) * nnz + fp * n + 7 * fp * m
+    raise ValueError(kind)
+
+
+def ncu_traffic(kernel: str):
+    """dram bytes per launch from the committed ncu summary, if any."""
+    f = ROOT / "profiles" / "traffic_config1.txt"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        parts = line.split()
+        if len(parts) == 3 and parts[0] == "traffic_bytes_per_launch" and parts[1] == kernel:
+            return float(parts[2])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"mc_clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        self.path.unlink(missing_ok=True)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def init_dist(world: int, backend: str):
+    if world <= 1:
+        return None
+    import datetime
+    import torch.distributed as dist
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=600))
+    return dist
+
+
+def max_over_ranks(dist, value: float, device) -> float:
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(dist, value: float, device) -> float:
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def make_model(seed: int):
+    from mcpdlp import generators
+    w = WORKLOAD
+    return generators.random_lp(seed, w["m"], w["n"], w["k"])
+
+
+def cpu_reference_sample(model, warmup_runs: int = 1, timed_runs: int = 1, iters: int = 40) -> dict:
+    """The reference CPU solve_pdlp on the same LP: setup-only runs and
+    `iters`-iteration runs; steady iterations/s = iters / (T_iters - T_setup)."""
+    from oracle import ReferencePdlp, OraclePort
+    from mcpdlp import _abi
+    if ReferencePdlp.available():
+        solver, kind = ReferencePdlp(), "reference"
+    else:
+        solver, kind = OraclePort(), "port"
+    o = _abi.default_options_struct()
+    o.primal_tolerance = o.dual_tolerance = o.gap_tolerance = TOL
+    t_setup = []
+    for _ in range(max(1, warmup_runs)):
+        o.max_iterations = 0
+        t0 = time.perf_counter()
+        solver.solve(model, o)
+        t_setup.append(time.perf_counter() - t0)
+    t_run = []
+    for _ in range(max(1, timed_runs)):
+        o.max_iterations = iters
+        t0 = time.perf_counter()
+        r = solver.solve(model, o)
+        t_run.append(time.perf_counter() - t0)
+    setup = float(np.median(t_setup))
+    per_iter = max(1e-9, (float(np.median(t_run)) - setup) / iters)
+    return dict(value=1.0 / per_iter, unit=UNIT, cores=1, kind=kind,
+                sample=(f"reference solve_pdlp on the same 2M x 5M LP (40M nnz): "
+                        f"{len(t_setup)} setup-only solves (max_iterations=0, {setup:.2f} s) and "
+                        f"{len(t_run)} solves of {iters} iterations; steady rate = {iters} / "
+                        f"(T_{iters} - T_0)"),
+                setup_s=setup, ms_per_iteration=per_iter * 1e3, last_primal=r.primal_infeasibility)
+
+
+def run_reference_arm(args) -> None:
+    world, rank, local = dist_env()
+    if rank != 0:
+        return
+    model = make_model(WORKLOAD["seed"])
+    t0 = time.perf_counter()
+    sample = cpu_reference_sample(model, warmup_runs=max(1, args.warmup), timed_runs=max(1, args.steps))
+    wall = time.perf_counter() - t0
+    line = {
+        "metric": METRIC, "value": sample["value"], "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sample["ms_per_iteration"] * 40,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator, known optimum)", "impl": "reference",
+        "config": dict(workload="synthetic LP m=2M n=5M 8 nnz/col (40M nnz), FP64, Ruiz 10 passes, "
+                                "tolerance 1e-8", m=WORKLOAD["m"], n=WORKLOAD["n"],
+                       nnz=WORKLOAD["n"] * WORKLOAD["k"], seed=WORKLOAD["seed"],
+                       step="40 PDHG iterations of the reference CPU PDLP (setup excluded)"),
+        "cpu_baseline": {k: sample[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": sample["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": wall,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_engine_arm(args) -> None:
+    import torch
+    import mcpdlp
+    from mcpdlp import PdlpOptions
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = init_dist(world, "nccl")
+
+    model = make_model(WORKLOAD["seed"])
+    m, n, nnz = model.num_rows, model.num_cols, model.nnz
+    ctx = mcpdlp.Context(local)
+    dmodel = mcpdlp.DeviceModel(model, f"cuda:{local}")
+    x = torch.empty(n, dtype=torch.float64, device=dev)
+    y = torch.empty(m, dtype=torch.float64, device=dev)
+    opts = PdlpOptions(device=local)
+    opts.set_tolerance(TOL)
+
+    # warm-up solves (also the graph capture / arena allocation)
+    for _ in range(args.warmup):
+        ctx.solve_device(dmodel, opts, x, y)
+    torch.cuda.synchronize()
+
+    # ---- value: device-resident inputs
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    results = []
+    stream = torch.cuda.current_stream()
+    with ClockSampler(local) as clocks:
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        t_host0 = time.perf_counter()
+        for _ in range(args.steps):
+            results.append(ctx.solve_device(dmodel, opts, x, y))
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        t_host = time.perf_counter() - t_host0
+    clock = clocks.summary()
+    # the engine runs on its own stream and every solve synchronises it before
+    # returning, so the host interval brackets exactly the device work; the
+    # torch events bracket the same interval on the caller's stream
+    dev_ms = max(ev0.elapsed_time(ev1), 0.0)
+    elapsed_s = max(t_host, dev_ms / 1e3)
+    if dist:
+        dist.barrier()
+    iters = sum(r.iterations for r in results)
+    launches = sum(r.extra["kernel_launches"] for r in results)
+    t_max = max_over_ranks(dist, elapsed_s, dev)
+    iters_all = sum_over_ranks(dist, float(iters), dev)
+    value = iters_all / t_max
+    last = results[-1]
+
+    # ---- e2e: host buffers through the public API (copies in the timed region)
+    pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
+    hmodel = mcpdlp.Model(m, n, pin(model.col_start), pin(model.row_index), pin(model.value),
+                          pin(model.objective), pin(model.var_lower), pin(model.var_upper),
+                          pin(model.row_lower), pin(model.row_upper))
+    ctx.solve(hmodel, opts)  # warm
+    if dist:
+        dist.barrier()
+    e2e_res = []
+    t0 = time.perf_counter()
+    for _ in range(max(1, args.steps)):
+        e2e_res.append(ctx.solve(hmodel, opts))
+    e2e_s = time.perf_counter() - t0
+    e2e_t = max_over_ranks(dist, e2e_s, dev)
+    e2e_iters = sum_over_ranks(dist, float(sum(r.iterations for r in e2e_res)), dev)
+    h2d_bytes = (4 * (n + 1) + 12 * nnz + 8 * 3 * n + 8 * 2 * m)
+    d2h_bytes = 8 * (n + m)
+
+    # ---- roofline of the dominant kernel: a profiled solve (events per launch)
+    popts = PdlpOptions(device=local, profile_kernels=True)
+    popts.set_tolerance(TOL)
+    prof = ctx.solve_device(dmodel, popts, x, y)
+    kms = prof.extra["kernel_ms_by_kind"]
+    kl = prof.extra["launches_by_kind"]
+    per_launch = {k: kms[k] / kl[k] for k in ("primal", "dual") if kl.get(k)}
+    dominant = max(("primal", "dual"), key=lambda k: kms.get(k, 0.0))
+    algo = kernel_bytes(dominant, m, n, nnz)
+    achieved = algo / (per_launch[dominant] / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    traffic = ncu_traffic(dominant)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "kernel": f"k_{dominant}",
+                "peak_source": peak_kind, "algorithmic_bytes_per_launch": algo,
+                "ms_per_launch": per_launch[dominant],
+                "other_kernel": {k: {"ms_per_launch": v,
+                                     "achieved_gbs": kernel_bytes(k, m, n, nnz) / (v / 1e3) / 1e9}
+                                 for k, v in per_launch.items() if k != dominant},
+                "time_share": {k: kms[k] / max(1e-9, sum(kms.values())) for k in kms if kms[k] > 0}}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max * 1e3 / max(1, args.steps),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator, known optimum)",
+        "config": dict(workload="synthetic LP m=2M n=5M 8 nnz/col (40M nnz), FP64, Ruiz 10 passes, "
+                                "tolerance 1e-8", m=m, n=n, nnz=nnz, seed=WORKLOAD["seed"],
+                       step="one full PDLP solve to 1e-8 relative KKT (replica per rank)",
+                       l2="inputs larger than L2 (960 MB of matrix per iteration)",
+                       parallelism=f"replicas x{world}"),
+        "time_to_tol_s": t_max / max(1, args.steps),
+        "iterations_to_tol": last.iterations,
+        "status": last.status.name,
+        "objective": last.objective,
+        "objective_rel_err_vs_analytic": abs(last.objective - model.info["optimum"]) / abs(model.info["optimum"]),
+        "kkt": {"primal": last.primal_infeasibility, "dual": last.dual_infeasibility, "gap": last.duality_gap},
+        "clocks": clock,
+        "gpu_launches": launches,
+        "e2e": {"value": e2e_iters / e2e_t, "unit": UNIT, "h2d_bytes_per_step": h2d_bytes,
+                "d2h_bytes_per_step": d2h_bytes, "s_per_step": e2e_t / max(1, args.steps)},
+        "roofline": roofline,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_reference_sample(model)
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_engine_arm(args)
+
+
+if __name__ == "__main__":
+    main()

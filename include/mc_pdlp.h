@@ -1,0 +1,243 @@
+/*
+ * mc_pdlp.h -- C ABI of the B200 (sm_100a) PDLP engine.
+ *
+ * This is the boundary a host solver binds to.  It replaces, for the GPU
+ * backend, the reference entry
+ *     PdlpResult solve_pdlp(const model::Model&, const PdlpOptions&)
+ *     (include/markov_cero/lp/first_order/pdlp.hpp:67, src/lp/first_order/pdlp.cpp:139)
+ * with plain pointers and sizes: no C++ types, no exceptions, an int status on
+ * every call.  Options and results mirror PdlpOptions (pdlp.hpp:18-41) and
+ * PdlpResult (pdlp.hpp:45-63) field by field; fields the reference does not
+ * have are grouped at the end of each struct and say so.
+ *
+ * Model layout (model.hpp:25-34, 53-70): CSC with int32 column pointers and
+ * row indices (rows strictly increasing within a column, values finite and
+ * nonzero, exactly what SparseMatrixCSC::validate accepts, model.cpp:41-66)
+ * and +-INFINITY in place of BoundKind::{negative,positive}_infinity.
+ *
+ * Threading: calls on different contexts may run concurrently from different
+ * host threads; one context must not be used by two threads at once.
+ * Errors: every function returns MC_OK (0) or an mc_error code; the text of
+ * the last error on the calling thread is available from mc_last_error().
+ * There is no CPU fallback: without a usable sm_100 device every solve
+ * returns MC_ERR_NO_DEVICE.
+ */
+#ifndef MC_PDLP_H
+#define MC_PDLP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MC_PDLP_ABI_VERSION 1
+
+/* Return codes of every entry point. The CLI of the reference maps
+ * std::invalid_argument -> InvalidModel, std::length_error -> ResourceLimit and
+ * anything else -> NumericalFailure (apps/markov_cero_solve.cpp:418-434); the
+ * codes below keep those three classes apart. */
+typedef enum mc_error {
+    MC_OK = 0,
+    MC_ERR_INVALID_ARGUMENT = 1, /* malformed model/options (invalid_argument) */
+    MC_ERR_NO_DEVICE = 2,        /* no CUDA device, or not sm_100             */
+    MC_ERR_OUT_OF_MEMORY = 3,    /* device allocation failed                  */
+    MC_ERR_RESOURCE_LIMIT = 4,   /* sizes beyond the engine's index range     */
+    MC_ERR_CUDA = 5,             /* any other CUDA runtime error              */
+    MC_ERR_INTERNAL = 6
+} mc_error;
+
+/* PdlpStatus, same order (pdlp.hpp:43). */
+typedef enum mc_pdlp_status {
+    MC_PDLP_OPTIMAL = 0,
+    MC_PDLP_ITERATION_LIMIT = 1,
+    MC_PDLP_INFEASIBLE_OR_UNBOUNDED = 2,
+    MC_PDLP_NUMERICAL_FAILURE = 3
+} mc_pdlp_status;
+
+enum { MC_BACKEND_CPU = 0, MC_BACKEND_GPU = 1 };                 /* pdlp.hpp:15 */
+enum { MC_RESTART_NONE = 0, MC_RESTART_ADAPTIVE = 1, MC_RESTART_FIXED = 2 }; /* pdlp.hpp:16 */
+enum { MC_MINIMIZE = 0, MC_MAXIMIZE = 1 };                       /* model.hpp:11 */
+enum { MC_MEMORY_HOST = 0, MC_MEMORY_DEVICE = 1 };
+enum { MC_PRECISION_FP64 = 0, MC_PRECISION_FP32_REFINE = 1 };
+
+/* An LP in the reference's Model shape (model.hpp:53-70).  `memory` says
+ * where every array lives; device arrays must belong to the context's
+ * device.  The engine never writes to these arrays. */
+typedef struct mc_lp {
+    int32_t num_rows;            /* m */
+    int32_t num_cols;            /* n */
+    int64_t nnz;
+    const int32_t* col_start;    /* [n+1], col_start[0] = 0, col_start[n] = nnz */
+    const int32_t* row_index;    /* [nnz] */
+    const double* value;         /* [nnz] */
+    const double* objective;     /* [n] */
+    const double* var_lower;     /* [n], -INFINITY = unbounded below */
+    const double* var_upper;     /* [n], +INFINITY = unbounded above */
+    const double* row_lower;     /* [m] */
+    const double* row_upper;     /* [m] */
+    double objective_offset;
+    int32_t objective_sense;     /* MC_MINIMIZE / MC_MAXIMIZE */
+    int32_t memory;              /* MC_MEMORY_HOST / MC_MEMORY_DEVICE */
+} mc_lp;
+
+/* PdlpOptions (pdlp.hpp:18-41). Defaults from mc_pdlp_default_options(). */
+typedef struct mc_pdlp_options {
+    int64_t max_iterations;           /* 100000 */
+    int64_t restart_every;            /* 40 */
+    double primal_tolerance;          /* 1e-4 */
+    double dual_tolerance;            /* 1e-4 */
+    double gap_tolerance;             /* 1e-4 */
+    double step_size_reduction;       /* 0.9 (initial eta) */
+    int64_t power_iterations;         /* 20, unused (as in the reference) */
+    int32_t backend;                  /* MC_BACKEND_GPU; MC_BACKEND_CPU is rejected */
+    int32_t restart_strategy;         /* MC_RESTART_ADAPTIVE */
+    double restart_reduction_factor;  /* 0.368 */
+    int32_t adaptive_step_size;       /* 1 */
+    int32_t adaptive_primal_weight;   /* 1 */
+    double initial_primal_weight;     /* 0 = derive from ||c|| / ||b|| */
+    double primal_weight_smoothing;   /* 0.5 */
+    int32_t ruiz_scaling;             /* 1 */
+    int64_t ruiz_iterations;          /* 10 */
+    /* ---- engine extensions, no counterpart in PdlpOptions ---- */
+    int32_t precision;                /* MC_PRECISION_FP64 */
+    int32_t device;                   /* CUDA ordinal used by mc_pdlp_solve, default 0 */
+    int32_t profile_kernels;          /* 1: time every kernel launch with CUDA events
+                                         (no CUDA graph; slower); fills kernel_ms_by_kind */
+    int32_t refine_max_rounds;        /* FP32_REFINE: outer refinement rounds, default 12 */
+    double refine_inner_tolerance;    /* FP32_REFINE: inner relative KKT target, default 1e-4 */
+    int32_t check_every_chunks;       /* host status poll interval in restart chunks, default 1 */
+    int32_t reserved_i[7];
+    double reserved_d[8];
+} mc_pdlp_options;
+
+enum {
+    MC_KERNEL_PRIMAL = 0,    /* A^T y SpMV + primal prox + averages           */
+    MC_KERNEL_DUAL = 1,      /* A x-bar SpMV + dual prox + averages           */
+    MC_KERNEL_DUAL_STEP = 2, /* A x-bar and A dx SpMV on step-size iterations */
+    MC_KERNEL_RESIDUAL = 3,  /* KKT residual SpMVs + reductions + restart     */
+    MC_KERNEL_SETUP = 4,     /* transpose, Ruiz, norms                        */
+    MC_KERNEL_OTHER = 5,
+    MC_KERNEL_KINDS = 8
+};
+
+/* PdlpResult (pdlp.hpp:45-63).  primal/dual are returned through separate
+ * caller-owned buffers (see mc_pdlp_solve). */
+typedef struct mc_pdlp_result {
+    int32_t status;                   /* mc_pdlp_status */
+    double objective;
+    double primal_infeasibility;
+    double dual_infeasibility;
+    double duality_gap;
+    double tolerance;
+    int64_t iterations;
+    char message[160];
+    double h2d_ms;
+    double kernel_ms;
+    double d2h_ms;
+    double total_ms;
+    char backend_actually_used[16];   /* "cuda" */
+    /* ---- engine extensions ---- */
+    int64_t ruiz_iterations_executed;
+    int64_t restarts;
+    double final_primal_weight;
+    double final_step_size;           /* eta */
+    int64_t refinement_rounds;        /* FP32_REFINE only */
+    int64_t inner_iterations;         /* FP32_REFINE: PDHG iterations over all rounds */
+    double kernel_ms_by_kind[MC_KERNEL_KINDS];
+    int64_t launches_by_kind[MC_KERNEL_KINDS];
+    int64_t kernel_launches;          /* engine kernels launched by this solve */
+    double reserved_d[4];
+} mc_pdlp_result;
+
+/* Optional per-check history (one entry per restart check). */
+typedef struct mc_pdlp_trace {
+    int64_t capacity;   /* entries available in every array below */
+    int64_t count;      /* entries written */
+    int64_t* iteration;
+    double* primal_infeasibility;
+    double* dual_infeasibility;
+    double* duality_gap;
+    double* step_size;       /* eta after the check */
+    double* primal_weight;   /* omega after the check */
+    int32_t* restarted;
+} mc_pdlp_trace;
+
+typedef struct mc_pdlp_ctx mc_pdlp_ctx;
+
+int mc_pdlp_abi_version(void);
+void mc_pdlp_default_options(mc_pdlp_options* options);
+
+/* sizeof of mc_lp, mc_pdlp_options, mc_pdlp_result, mc_pdlp_trace (in that
+ * order) into sizes[0..count-1]; lets bindings check their struct layouts. */
+int mc_pdlp_struct_sizes(size_t* sizes, int count);
+
+/* Thread-local text of the last failure ("" if none). Returns MC_OK. */
+int mc_last_error(char* buffer, size_t length);
+
+/* Number of usable sm_100 devices (0 if none). */
+int mc_device_count(int* count);
+
+/* A context owns a device, a stream and reusable device buffers; keeping one
+ * alive across solves avoids repeated allocation. */
+int mc_pdlp_ctx_create(int device, mc_pdlp_ctx** out);
+int mc_pdlp_ctx_destroy(mc_pdlp_ctx* ctx);
+
+/*
+ * Solve one LP with PDLP on the GPU.  Same algorithm, options, statuses and
+ * result fields as the reference solve_pdlp (src/lp/first_order/pdlp.cpp:139-276):
+ * Ruiz equilibration, diagonal steps, adaptive step size, adaptive restarts
+ * to the average, adaptive primal weight, relative KKT termination on the
+ * unscaled averages, checked every restart_every iterations.
+ *   initial_primal / initial_dual: optional warm start in the original space
+ *     (NULL = the reference start x = proj(0), y = 0); an extension.
+ *   primal_out[n] / dual_out[m]: caller-owned, in lp->memory space; receive the
+ *     unscaled average iterates, like PdlpResult::primal / dual.  May be NULL.
+ *   trace: optional history, may be NULL.
+ * Non-convergence is a status, not an error.
+ */
+int mc_pdlp_ctx_solve(mc_pdlp_ctx* ctx, const mc_lp* lp, const mc_pdlp_options* options,
+                      const double* initial_primal, const double* initial_dual,
+                      double* primal_out, double* dual_out,
+                      mc_pdlp_result* result, mc_pdlp_trace* trace);
+
+/* One-shot form: a temporary context on options->device. */
+int mc_pdlp_solve(const mc_lp* lp, const mc_pdlp_options* options,
+                  const double* initial_primal, const double* initial_dual,
+                  double* primal_out, double* dual_out, mc_pdlp_result* result);
+
+/*
+ * Kernel-level entry points (device pointers, the context's stream), used by
+ * the parity tests and the roofline measurement.  They replace the reference's
+ * file-local helpers of the same meaning.
+ */
+
+/* y = A x over CSR (row_start[m+1], col_index, value); the reference computes
+ * it as a CSC scatter, spmv() at src/lp/first_order/pdlp.cpp:22-32. */
+int mc_spmv_csr(mc_pdlp_ctx* ctx, int32_t m, int32_t n, const int32_t* row_start,
+                const int32_t* col_index, const double* value, const double* x, double* y);
+
+/* Build CSR(A) from CSC(A) on the device, rows' entries in ascending column
+ * order; the reference keeps only CSC.  row_start[m+1], col_index[nnz],
+ * value[nnz] are caller-allocated device arrays. */
+int mc_csc_to_csr(mc_pdlp_ctx* ctx, int32_t m, int32_t n, int64_t nnz,
+                  const int32_t* col_start, const int32_t* row_index, const double* value,
+                  int32_t* row_start, int32_t* col_index, double* csr_value);
+
+/* Ruiz equilibration of a device-resident model in place (values of both
+ * copies, bounds, objective), equilibrate_model at
+ * src/scale/ruiz_scaling.cpp:152-247.  row_scale[m], col_scale[n] receive D_R,
+ * D_C; *iterations_executed the pass count. */
+int mc_ruiz_equilibrate(mc_pdlp_ctx* ctx, int32_t m, int32_t n, int64_t nnz,
+                        const int32_t* col_start, const int32_t* row_index, double* csc_value,
+                        const int32_t* row_start, const int32_t* col_index, double* csr_value,
+                        double* objective, double* var_lower, double* var_upper,
+                        double* row_lower, double* row_upper, int64_t max_iterations,
+                        double* row_scale, double* col_scale, int64_t* iterations_executed);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MC_PDLP_H */

@@ -1,0 +1,300 @@
+// Host driver of the B200 PDLP engine and the C ABI of include/mc_pdlp.h.
+//
+// A solve (the GPU form of solve_pdlp, src/lp/first_order/pdlp.cpp:139-276):
+//   1. copy the model into the context's arena (one allocation, reused);
+//   2. validate it on the device (every later gather stays in bounds);
+//   3. build CSR(A) from CSC(A) on the device, rows in ascending column order;
+//   4. Ruiz equilibration of both copies (ruiz_scaling.cpp:152-247);
+//   5. norms, step sizes and the starting point;
+//   6. the PDHG loop in chunks of restart_every iterations, each chunk one
+//      CUDA graph replay (2 fused SpMV kernels per iteration plus the
+//      step-size probe every 10th iteration, then the KKT residual pass and
+//      the restart logic, all on the device); the host polls one flag per
+//      chunk, one chunk behind, so the GPU never idles between chunks;
+//   7. unscale the averages and copy them out.
+#include "mc_pdlp.h"
+#include "mc_pdlp_testing.h"
+
+#include "engine.hpp"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+namespace mc {
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string g_error;
+static int g_inject_alloc_failures = 0;
+
+int set_error(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_error = buf;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what, int line) {
+    const int code = (e == cudaErrorMemoryAllocation) ? MC_ERR_OUT_OF_MEMORY
+                     : (e == cudaErrorNoDevice || e == cudaErrorInvalidDevice ||
+                        e == cudaErrorInsufficientDriver || e == cudaErrorNoKernelImageForDevice)
+                         ? MC_ERR_NO_DEVICE
+                         : MC_ERR_CUDA;
+    return set_error(code, "%s failed at engine.cu:%d: %s", what, line, cudaGetErrorString(e));
+}
+
+int check_device(int device) {
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0)
+        return set_error(MC_ERR_NO_DEVICE, "no CUDA device (%s); the engine has no CPU fallback",
+                         e == cudaSuccess ? "count 0" : cudaGetErrorString(e));
+    if (device < 0 || device >= count)
+        return set_error(MC_ERR_NO_DEVICE, "device %d out of range (%d devices)", device, count);
+    cudaDeviceProp prop;
+    CU(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10)
+        return set_error(MC_ERR_NO_DEVICE, "device %d is sm_%d%d; this engine is built for sm_100a",
+                         device, prop.major, prop.minor);
+    return MC_OK;
+}
+
+// ----------------------------------------------------------------- arena
+int Arena::reserve(size_t bytes) {
+    if (bytes <= capacity) return MC_OK;
+    if (base) {
+        cudaFree(base);
+        base = nullptr;
+        capacity = 0;
+    }
+    if (g_inject_alloc_failures > 0) {
+        --g_inject_alloc_failures;
+        return set_error(MC_ERR_OUT_OF_MEMORY, "injected allocation failure (%zu bytes)", bytes);
+    }
+    cudaError_t e = cudaMalloc(&base, bytes);
+    if (e != cudaSuccess) {
+        base = nullptr;
+        cudaGetLastError();
+        return cuda_fail(e, "cudaMalloc(arena)", __LINE__);
+    }
+    capacity = bytes;
+    return MC_OK;
+}
+
+// ------------------------------------------------------------------ context
+Ctx::~Ctx() {
+    if (device >= 0) cudaSetDevice(device);
+    release_graphs();
+    if (arena.base) cudaFree(arena.base);
+    if (h_state) cudaFreeHost(h_state);
+    for (auto& e : prof_events) cudaEventDestroy(e);
+    for (cudaEvent_t e : {ev_a, ev_b, ev_c, ev_d, ev_poll[0], ev_poll[1]})
+        if (e) cudaEventDestroy(e);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+void Ctx::release_graphs() {
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+    graphs.clear();
+}
+
+int Ctx::init(int dev) {
+    TRY(check_device(dev));
+    device = dev;
+    CU(cudaSetDevice(dev));
+    CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    CU(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev));
+    CU(cudaEventCreate(&ev_a));
+    CU(cudaEventCreate(&ev_b));
+    CU(cudaEventCreate(&ev_c));
+    CU(cudaEventCreate(&ev_d));
+    CU(cudaEventCreateWithFlags(&ev_poll[0], cudaEventDisableTiming));
+    CU(cudaEventCreateWithFlags(&ev_poll[1], cudaEventDisableTiming));
+    CU(cudaMallocHost(reinterpret_cast<void**>(&h_state), sizeof(DevState) * 4));
+    return MC_OK;
+}
+
+// ------------------------------------------------------- launch bookkeeping
+void Ctx::begin_launch(int kind) {
+    launches[kind] += 1;
+    if (profiling && !capturing) {
+        if (prof_used + 2 > prof_events.size()) {
+            for (int q = 0; q < 64; ++q) {
+                cudaEvent_t e;
+                cudaEventCreate(&e);
+                prof_events.push_back(e);
+            }
+        }
+        cudaEventRecord(prof_events[prof_used], stream);
+        pending.push_back({kind, (int)prof_used});
+        prof_used += 2;
+    }
+}
+
+void Ctx::end_launch() {
+    if (profiling && !capturing) cudaEventRecord(prof_events[pending.back().first_event + 1], stream);
+}
+
+int Ctx::drain_profile() {
+    if (!profiling || pending.empty()) return MC_OK;
+    CU(cudaStreamSynchronize(stream));
+    for (const auto& p : pending) {
+        float ms = 0.f;
+        CU(cudaEventElapsedTime(&ms, prof_events[p.first_event], prof_events[p.first_event + 1]));
+        kernel_ms[p.kind] += ms;
+    }
+    pending.clear();
+    prof_used = 0;
+    return MC_OK;
+}
+
+int Ctx::launch_check(const char* what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, what, __LINE__);
+    return MC_OK;
+}
+
+int blocks_for(const Ctx& ctx, long long work_items, int per_block) {
+    long long b = (work_items + per_block - 1) / per_block;
+    const long long cap = std::min<long long>((long long)ctx.sm_count * (2048 / kBlock), kMaxPartials / 2);
+    if (b > cap) b = cap;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+int pick_lanes(double mean_len) {
+    const double half = mean_len / 2.0;
+    int g = 1;
+    while (g < 32 && 2.0 * g <= half) g *= 2;
+    return g;
+}
+
+int solve_fp32_refine(Ctx&, const mc_lp*, const mc_pdlp_options*, const double*, const double*,
+                      double*, double*, mc_pdlp_result*, mc_pdlp_trace*) {
+    return set_error(MC_ERR_INVALID_ARGUMENT, "MC_PRECISION_FP32_REFINE is not available in this build");
+}
+
+}  // namespace mc
+
+#include "solve.cuh"
+#include "kernel_api.cuh"
+
+using namespace mc;
+
+// =================================================================== C ABI
+extern "C" {
+
+int mc_pdlp_abi_version(void) { return MC_PDLP_ABI_VERSION; }
+
+void mc_pdlp_default_options(mc_pdlp_options* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof *o);
+    o->max_iterations = 100000;
+    o->restart_every = 40;
+    o->primal_tolerance = 1e-4;
+    o->dual_tolerance = 1e-4;
+    o->gap_tolerance = 1e-4;
+    o->step_size_reduction = 0.9;
+    o->power_iterations = 20;
+    o->backend = MC_BACKEND_GPU;
+    o->restart_strategy = MC_RESTART_ADAPTIVE;
+    o->restart_reduction_factor = 0.368;
+    o->adaptive_step_size = 1;
+    o->adaptive_primal_weight = 1;
+    o->initial_primal_weight = 0.0;
+    o->primal_weight_smoothing = 0.5;
+    o->ruiz_scaling = 1;
+    o->ruiz_iterations = 10;
+    o->precision = MC_PRECISION_FP64;
+    o->device = 0;
+    o->profile_kernels = 0;
+    o->refine_max_rounds = 12;
+    o->refine_inner_tolerance = 1e-4;
+    o->check_every_chunks = 1;
+}
+
+int mc_pdlp_struct_sizes(size_t* sizes, int count) {
+    const size_t all[4] = {sizeof(mc_lp), sizeof(mc_pdlp_options), sizeof(mc_pdlp_result), sizeof(mc_pdlp_trace)};
+    if (!sizes || count < 0) return set_error(MC_ERR_INVALID_ARGUMENT, "bad sizes buffer");
+    for (int q = 0; q < count && q < 4; ++q) sizes[q] = all[q];
+    return MC_OK;
+}
+
+int mc_last_error(char* buffer, size_t length) {
+    if (buffer && length) std::snprintf(buffer, length, "%s", g_error.c_str());
+    return MC_OK;
+}
+
+int mc_device_count(int* count) {
+    if (!count) return set_error(MC_ERR_INVALID_ARGUMENT, "count is NULL");
+    *count = 0;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return MC_OK;
+    }
+    for (int d = 0; d < n; ++d) {
+        cudaDeviceProp p;
+        if (cudaGetDeviceProperties(&p, d) == cudaSuccess && p.major == 10) ++*count;
+    }
+    return MC_OK;
+}
+
+int mc_pdlp_ctx_create(int device, mc_pdlp_ctx** out) {
+    if (!out) return set_error(MC_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    auto* ctx = new (std::nothrow) Ctx();
+    if (!ctx) return set_error(MC_ERR_OUT_OF_MEMORY, "host allocation failed");
+    DeviceGuard guard(device);
+    const int rc = ctx->init(device);
+    if (rc != MC_OK) {
+        delete ctx;
+        return rc;
+    }
+    *out = reinterpret_cast<mc_pdlp_ctx*>(ctx);
+    return MC_OK;
+}
+
+int mc_pdlp_ctx_destroy(mc_pdlp_ctx* c) {
+    delete reinterpret_cast<Ctx*>(c);
+    return MC_OK;
+}
+
+int mc_pdlp_ctx_solve(mc_pdlp_ctx* c, const mc_lp* lp, const mc_pdlp_options* options,
+                      const double* initial_primal, const double* initial_dual, double* primal_out,
+                      double* dual_out, mc_pdlp_result* result, mc_pdlp_trace* trace) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(c);
+    if (!ctx) return set_error(MC_ERR_INVALID_ARGUMENT, "context is NULL");
+    DeviceGuard guard(ctx->device);
+    return solve_lp(*ctx, lp, options, initial_primal, initial_dual, primal_out, dual_out, result,
+                    trace);
+}
+
+int mc_pdlp_solve(const mc_lp* lp, const mc_pdlp_options* options, const double* initial_primal,
+                  const double* initial_dual, double* primal_out, double* dual_out,
+                  mc_pdlp_result* result) {
+    TRY(validate_options(options));
+    TRY(validate_lp(lp));
+    mc_pdlp_ctx* c = nullptr;
+    TRY(mc_pdlp_ctx_create(options->device, &c));
+    const int rc = mc_pdlp_ctx_solve(c, lp, options, initial_primal, initial_dual, primal_out,
+                                     dual_out, result, nullptr);
+    mc_pdlp_ctx_destroy(c);
+    return rc;
+}
+
+int mc_test_inject_alloc_failures(int count) {
+    g_inject_alloc_failures = count;
+    return MC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,467 @@
+// Per-iteration kernels of the PDHG loop (src/lp/first_order/pdlp.cpp:194-262).
+//
+// Every SpMV is fused with the vector update that consumes it, so one
+// iteration is two passes over the matrix: CSC (A^T y, the primal step) and
+// CSR (A x-bar, the dual step).  G lanes cooperate on one column/row ("vector
+// per row"; G = 32 is warp per row), chosen by the host from the mean line
+// length.  T is the storage/arithmetic type of the matrix and iterates
+// (double for the FP64 engine, float for the FP32 engine); every reduction
+// that feeds a decision (step size, KKT, restart) accumulates in double.
+#pragma once
+
+#include "common.cuh"
+
+namespace mc {
+
+// Pointers and sizes of one device-resident problem.
+template <class T>
+struct Iterates {
+    int m, n;
+    const int* csc_start;   // [n+1]
+    const int* csc_row;     // [nnz]
+    const T* csc_val;       // [nnz] scaled A, column major
+    const int* csr_start;   // [m+1]
+    const int* csr_col;     // [nnz]
+    const T* csr_val;       // [nnz] scaled A, row major
+    const T* c;             // [n] scaled objective (minimisation sign)
+    const T* lo;            // [n] scaled bounds, +-1e300 sentinels
+    const T* hi;
+    const T* blo;           // [m] scaled row bounds
+    const T* bhi;
+    const T* col_norm;      // [n] L1 norms of the scaled columns
+    const T* row_norm;      // [m]
+    T* x;                   // [n]
+    T* x_bar;               // [n]
+    T* x_avg;               // [n]
+    T* dx;                  // [n] step-size iterations only
+    T* y;                   // [m]
+    T* y_avg;               // [m]
+    T* ax_bar;              // [m] step-size iterations only
+    double* partials;       // [NUM_SLOTS * kMaxPartials]
+    DevState* st;
+};
+
+// Original-space data used by the residual pass (pdlp.cpp:62-135).
+struct Original {
+    const double* c;        // obj_sign * objective, unscaled
+    const double* obj;      // objective as given (primal objective :113-115)
+    const double* lo;       // variable bounds, sentinel form
+    const double* hi;
+    const double* blo;      // row bounds, sentinel form
+    const double* bhi;
+    const double* col_scale;
+    const double* row_scale;
+    double offset;
+};
+
+struct Controls {
+    double primal_tol, dual_tol, gap_tol;
+    double restart_reduction;
+    double weight_smoothing;
+    long long restart_every;
+    int strategy;          // 0 none, 1 adaptive, 2 fixed
+    int adaptive_step;
+    int adaptive_weight;
+};
+
+template <class T> __device__ __forceinline__ T mul_rn(T a, T b);
+template <> __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+template <> __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+template <class T> __device__ __forceinline__ T add_rn(T a, T b);
+template <> __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+template <> __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+template <class T> __device__ __forceinline__ T sub_rn(T a, T b);
+template <> __device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+template <> __device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+template <class T> __device__ __forceinline__ T div_rn(T a, T b);
+template <> __device__ __forceinline__ double div_rn(double a, double b) { return __ddiv_rn(a, b); }
+template <> __device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
+
+// Dot of line `j` of a compressed matrix with vector v, G lanes per line,
+// two independent accumulators per lane for memory-level parallelism.
+template <int G, class T>
+__device__ __forceinline__ T line_dot(const int* __restrict__ start, const int* __restrict__ idx,
+                                      const T* __restrict__ val, const T* __restrict__ v, int j,
+                                      bool valid, int sub) {
+    T s0 = T(0), s1 = T(0);
+    if (valid) {
+        const int b = start[j], e = start[j + 1];
+        int p = b + sub;
+        for (; p + G < e; p += 2 * G) {
+            const int i0 = __ldg(idx + p), i1 = __ldg(idx + p + G);
+            const T a0 = __ldg(val + p), a1 = __ldg(val + p + G);
+            s0 = fma(a0, v[i0], s0);
+            s1 = fma(a1, v[i1], s1);
+        }
+        if (p < e) s0 = fma(__ldg(val + p), v[__ldg(idx + p)], s0);
+    }
+    return group_sum<G>(s0 + s1);
+}
+
+// Two dots of the same line (A x-bar and A dx on step-size iterations).
+template <int G, class T>
+__device__ __forceinline__ void line_dot2(const int* __restrict__ start, const int* __restrict__ idx,
+                                          const T* __restrict__ val, const T* __restrict__ v,
+                                          const T* __restrict__ w, int j, bool valid, int sub,
+                                          T& out_v, T& out_w) {
+    T sv = T(0), sw = T(0);
+    if (valid) {
+        const int b = start[j], e = start[j + 1];
+        for (int p = b + sub; p < e; p += G) {
+            const int i = __ldg(idx + p);
+            const T a = __ldg(val + p);
+            sv = fma(a, v[i], sv);
+            sw = fma(a, w[i], sw);
+        }
+    }
+    out_v = group_sum<G>(sv);
+    out_w = group_sum<G>(sw);
+}
+
+// Plain y = A x over a compressed-row matrix (kernel-level entry point).
+template <int G, class T>
+__global__ void __launch_bounds__(kBlock) k_spmv(int rows, const int* __restrict__ start,
+                                                 const int* __restrict__ idx, const T* __restrict__ val,
+                                                 const T* __restrict__ x, T* __restrict__ y) {
+    constexpr int LPW = 32 / G;
+    const int lane = threadIdx.x & 31, sub = lane % G, slot = lane / G;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long t = warp; t * LPW < rows; t += nwarps) {
+        const int i = (int)(t * LPW) + slot;
+        const bool valid = i < rows;
+        const T s = line_dot<G>(start, idx, val, x, i, valid, sub);
+        if (valid && sub == 0) y[i] = s;
+    }
+}
+
+// ------------------------------------------------------------------ primal
+// g = c + A^T y; x+ = clamp(x - tau g, l, u); x-bar = 2x+ - x; x_avg update;
+// on step-size iterations also dx and sum col_norm dx^2  (pdlp.cpp:195-206, :226)
+template <int G, bool STEP, class T>
+__global__ void __launch_bounds__(kBlock) k_primal(Iterates<T> P, int k) {
+    __shared__ double scratch[32];
+    const DevState* st = P.st;
+    if (st->done) return;
+    const T step = T(st->eta / st->omega);          // tau_j = (eta/omega)/col_norm_j (:182)
+    const T cnt = T((double)(st->avg_count + k + 1));
+    constexpr int LPW = 32 / G;                      // lines per warp
+    const int lane = threadIdx.x & 31, sub = lane % G, slot = lane / G;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    double acc = 0.0;
+    for (long long t = warp; t * LPW < P.n; t += nwarps) {
+        const int j = (int)(t * LPW) + slot;
+        const bool valid = j < P.n;
+        const T aty = line_dot<G>(P.csc_start, P.csc_row, P.csc_val, P.y, j, valid, sub);
+        if (valid && sub == 0) {
+            const T g = add_rn(P.c[j], aty);
+            const T tau = div_rn(step, P.col_norm[j]);
+            const T xo = P.x[j];
+            const T xp = clampv(sub_rn(xo, mul_rn(tau, g)), P.lo[j], P.hi[j]);
+            const T d = sub_rn(xp, xo);
+            if (STEP) {
+                P.dx[j] = d;
+                const double cn = (double)P.col_norm[j];
+                acc += __dmul_rn(__dmul_rn(cn, (double)d), (double)d);
+            }
+            P.x[j] = xp;
+            P.x_bar[j] = sub_rn(mul_rn(T(2), xp), xo);
+            const T xa = P.x_avg[j];
+            P.x_avg[j] = add_rn(xa, div_rn(sub_rn(xp, xa), cnt));
+        }
+    }
+    if (STEP) {
+        acc = block_reduce(acc, scratch, OpSum());
+        if (threadIdx.x == 0) P.partials[SLOT_DX * kMaxPartials + blockIdx.x] = acc;
+    }
+}
+
+// ------------------------------------------------------------------- dual
+// v = y + sigma (A x-bar); y+ = v - sigma clamp(v/sigma, b_lo, b_hi); y_avg
+// (pdlp.cpp:220-224, :227)
+template <class T>
+__device__ __forceinline__ void dual_update(const Iterates<T>& P, int i, T ax, T sg, T cnt) {
+    const T sigma = div_rn(sg, P.row_norm[i]);
+    const T yo = P.y[i];
+    const T v = add_rn(yo, mul_rn(sigma, ax));
+    const T yn = sub_rn(v, mul_rn(sigma, clampv(div_rn(v, sigma), P.blo[i], P.bhi[i])));
+    P.y[i] = yn;
+    const T ya = P.y_avg[i];
+    P.y_avg[i] = add_rn(ya, div_rn(sub_rn(yn, ya), cnt));
+}
+
+template <int G, class T>
+__global__ void __launch_bounds__(kBlock) k_dual(Iterates<T> P, int k) {
+    const DevState* st = P.st;
+    if (st->done) return;
+    const T sg = T(st->eta * st->omega);             // sigma_i = (eta*omega)/row_norm_i (:183)
+    const T cnt = T((double)(st->avg_count + k + 1));
+    constexpr int LPW = 32 / G;
+    const int lane = threadIdx.x & 31, sub = lane % G, slot = lane / G;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long t = warp; t * LPW < P.m; t += nwarps) {
+        const int i = (int)(t * LPW) + slot;
+        const bool valid = i < P.m;
+        const T ax = line_dot<G>(P.csr_start, P.csr_col, P.csr_val, P.x_bar, i, valid, sub);
+        if (valid && sub == 0) dual_update(P, i, ax, sg, cnt);
+    }
+}
+
+// Step-size iteration, part 1: A x-bar (kept) and A dx -> sum (A dx)_i^2 / row_norm_i
+// (pdlp.cpp:207-210, :220).  The dual update waits for the new eta.
+template <int G, class T>
+__global__ void __launch_bounds__(kBlock) k_dual_probe(Iterates<T> P) {
+    __shared__ double scratch[32];
+    const DevState* st = P.st;
+    if (st->done) return;
+    constexpr int LPW = 32 / G;
+    const int lane = threadIdx.x & 31, sub = lane % G, slot = lane / G;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    double acc = 0.0;
+    for (long long t = warp; t * LPW < P.m; t += nwarps) {
+        const int i = (int)(t * LPW) + slot;
+        const bool valid = i < P.m;
+        T axb, adx;
+        line_dot2<G>(P.csr_start, P.csr_col, P.csr_val, P.x_bar, P.dx, i, valid, sub, axb, adx);
+        if (valid && sub == 0) {
+            P.ax_bar[i] = axb;
+            const double a = (double)adx;
+            acc += __ddiv_rn(__dmul_rn(a, a), (double)P.row_norm[i]);
+        }
+    }
+    acc = block_reduce(acc, scratch, OpSum());
+    if (threadIdx.x == 0) P.partials[SLOT_ADX * kMaxPartials + blockIdx.x] = acc;
+}
+
+// Step-size iteration, part 2: the adaptive eta rule (pdlp.cpp:207-219).
+__global__ void k_step_size(double* __restrict__ partials, int nprimal, int ndual, DevState* __restrict__ st,
+                            Controls ctl) {
+    __shared__ double scratch[32];
+    if (st->done) return;
+    const double dx_norm_sq = reduce_partials(partials + SLOT_DX * kMaxPartials, nprimal, scratch, OpSum());
+    const double adx_norm_sq = reduce_partials(partials + SLOT_ADX * kMaxPartials, ndual, scratch, OpSum());
+    if (threadIdx.x == 0 && ctl.adaptive_step && dx_norm_sq > 1e-14 && adx_norm_sq > 1e-14) {
+        const double L = sqrt(adx_norm_sq / dx_norm_sq);
+        if (L > 1e-6) {
+            const double target = 0.95 / L;
+            const double eta = st->eta;
+            if (target < eta) st->eta = maxv(0.1, maxv(target, eta * 0.8));
+            else if (target > 1.05 * eta && eta < 0.99) st->eta = minv(0.99, eta * 1.05);
+        }
+    }
+}
+
+// Step-size iteration, part 3: the dual update from the kept A x-bar.
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_dual_apply(Iterates<T> P, int k) {
+    const DevState* st = P.st;
+    if (st->done) return;
+    const T sg = T(st->eta * st->omega);
+    const T cnt = T((double)(st->avg_count + k + 1));
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.m; i += gridDim.x * blockDim.x)
+        dual_update(P, i, P.ax_bar[i], sg, cnt);
+}
+
+// --------------------------------------------------------------- residuals
+// compute_unscaled_residuals (pdlp.cpp:62-135) over the averages, row part:
+// (A x_avg)_i unscaled, relative row violation (max), row part of the dual
+// objective (sum).  Always FP64 (the FP32 engine evaluates its FP32 averages
+// through double gathers).
+template <int G, class T>
+__global__ void __launch_bounds__(kBlock) k_residual_rows(Iterates<T> P, Original O) {
+    __shared__ double scratch[32];
+    const DevState* st = P.st;
+    if (st->done) return;
+    constexpr int LPW = 32 / G;
+    const int lane = threadIdx.x & 31, sub = lane % G, slot = lane / G;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    double vmax = 0.0, dsum = 0.0, bad = 0.0;
+    for (long long t = warp; t * LPW < P.m; t += nwarps) {
+        const int i = (int)(t * LPW) + slot;
+        const bool valid = i < P.m;
+        double s = 0.0;
+        if (valid) {
+            const int b = P.csr_start[i], e = P.csr_start[i + 1];
+            for (int p = b + sub; p < e; p += G)
+                s = fma((double)P.csr_val[p], (double)P.x_avg[P.csr_col[p]], s);
+        }
+        s = group_sum<G>(s);
+        if (valid && sub == 0) {
+            const double ax = __ddiv_rn(s, O.row_scale[i]);
+            const double lo = O.blo[i], hi = O.bhi[i];
+            const double proj = clampv(ax, lo, hi);
+            const double r = fabs(ax - proj);
+            const double sc = 1.0 + maxv(fabs(ax), fabs(proj) < 1e299 ? fabs(proj) : 0.0);
+            vmax = maxv(vmax, r / sc);
+            const double yu = __dmul_rn((double)P.y_avg[i], O.row_scale[i]);
+            if (yu > 0.0 && hi < 1e299) dsum -= __dmul_rn(yu, hi);
+            else if (yu < 0.0 && lo > -1e299) dsum -= __dmul_rn(yu, lo);
+            if (!isfinite(ax) || !isfinite(yu)) bad += 1.0;
+        }
+    }
+    vmax = block_reduce(vmax, scratch, OpMax());
+    if (threadIdx.x == 0) P.partials[SLOT_ROW_MAX * kMaxPartials + blockIdx.x] = vmax;
+    dsum = block_reduce(dsum, scratch, OpSum());
+    if (threadIdx.x == 0) P.partials[SLOT_ROW_DOBJ * kMaxPartials + blockIdx.x] = dsum;
+    bad = block_reduce(bad, scratch, OpSum());
+    if (threadIdx.x == 0) P.partials[SLOT_NAN * kMaxPartials + blockIdx.x] = bad;
+}
+
+// Column part: (A^T y_avg)_j unscaled, bound violation (max), squared dual
+// residual (sum), primal objective (sum), column part of the dual objective.
+template <int G, class T>
+__global__ void __launch_bounds__(kBlock) k_residual_cols(Iterates<T> P, Original O) {
+    __shared__ double scratch[32];
+    const DevState* st = P.st;
+    if (st->done) return;
+    constexpr int LPW = 32 / G;
+    const int lane = threadIdx.x & 31, sub = lane % G, slot = lane / G;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    double vmax = 0.0, dres = 0.0, pobj = 0.0, dobj = 0.0, bad = 0.0;
+    for (long long t = warp; t * LPW < P.n; t += nwarps) {
+        const int j = (int)(t * LPW) + slot;
+        const bool valid = j < P.n;
+        double s = 0.0;
+        if (valid) {
+            const int b = P.csc_start[j], e = P.csc_start[j + 1];
+            for (int p = b + sub; p < e; p += G)
+                s = fma((double)P.csc_val[p], (double)P.y_avg[P.csc_row[p]], s);
+        }
+        s = group_sum<G>(s);
+        if (valid && sub == 0) {
+            const double aty = __ddiv_rn(s, O.col_scale[j]);
+            const double xu = __dmul_rn((double)P.x_avg[j], O.col_scale[j]);
+            const double lo = O.lo[j], hi = O.hi[j];
+            const double proj = clampv(xu, lo, hi);
+            const double r = fabs(xu - proj);
+            const double sc = 1.0 + maxv(fabs(xu), fabs(proj) < 1e299 ? fabs(proj) : 0.0);
+            vmax = maxv(vmax, r / sc);
+            const double g = __dadd_rn(O.c[j], aty);
+            const double xp = clampv(__dsub_rn(xu, g), lo, hi);
+            const double diff = __dsub_rn(xu, xp);
+            dres += __dmul_rn(diff, diff);
+            pobj += __dmul_rn(O.obj[j], xu);
+            if (g > 0.0 && lo > -1e299) dobj += __dmul_rn(g, lo);
+            else if (g < 0.0 && hi < 1e299) dobj += __dmul_rn(g, hi);
+            if (!isfinite(xu) || !isfinite(g)) bad += 1.0;
+        }
+    }
+    vmax = block_reduce(vmax, scratch, OpMax());
+    if (threadIdx.x == 0) P.partials[SLOT_COL_MAX * kMaxPartials + blockIdx.x] = vmax;
+    dres = block_reduce(dres, scratch, OpSum());
+    if (threadIdx.x == 0) P.partials[SLOT_COL_DRES * kMaxPartials + blockIdx.x] = dres;
+    pobj = block_reduce(pobj, scratch, OpSum());
+    if (threadIdx.x == 0) P.partials[SLOT_COL_POBJ * kMaxPartials + blockIdx.x] = pobj;
+    dobj = block_reduce(dobj, scratch, OpSum());
+    if (threadIdx.x == 0) P.partials[SLOT_COL_DOBJ * kMaxPartials + blockIdx.x] = dobj;
+    bad = block_reduce(bad, scratch, OpSum());
+    if (threadIdx.x == 0) P.partials[(SLOT_NAN + 0) * kMaxPartials + kMaxPartials / 2 + blockIdx.x] = bad;
+}
+
+// Device trace of the restart checks (optional).
+struct TraceBuf {
+    long long capacity;
+    long long* iteration;
+    double* primal;
+    double* dual;
+    double* gap;
+    double* eta;
+    double* omega;
+    int* restarted;
+};
+
+// Restart check (pdlp.cpp:229-261): KKT scalars, termination, adaptive
+// restart, primal weight.  `span` = iterations in the chunk just finished;
+// `final_pass` = evaluate only (loop exhausted, :263-275).
+__global__ void k_finalize(double* __restrict__ partials, int nrow_parts, int ncol_parts, long long span,
+                           int final_pass, double offset, Controls ctl, TraceBuf tr,
+                           DevState* __restrict__ st) {
+    __shared__ double scratch[32];
+    if (st->done) return;
+    const double row_max = reduce_partials(partials + SLOT_ROW_MAX * kMaxPartials, nrow_parts, scratch, OpMax());
+    const double row_dobj = reduce_partials(partials + SLOT_ROW_DOBJ * kMaxPartials, nrow_parts, scratch, OpSum());
+    const double col_max = reduce_partials(partials + SLOT_COL_MAX * kMaxPartials, ncol_parts, scratch, OpMax());
+    const double col_dres = reduce_partials(partials + SLOT_COL_DRES * kMaxPartials, ncol_parts, scratch, OpSum());
+    const double col_pobj = reduce_partials(partials + SLOT_COL_POBJ * kMaxPartials, ncol_parts, scratch, OpSum());
+    const double col_dobj = reduce_partials(partials + SLOT_COL_DOBJ * kMaxPartials, ncol_parts, scratch, OpSum());
+    const double bad_rows = reduce_partials(partials + SLOT_NAN * kMaxPartials, nrow_parts, scratch, OpSum());
+    const double bad_cols = reduce_partials(partials + SLOT_NAN * kMaxPartials + kMaxPartials / 2, ncol_parts,
+                                            scratch, OpSum());
+    if (threadIdx.x != 0) return;
+    const double primal = maxv(row_max, col_max);
+    const double dual = sqrt(col_dres) / st->c_scale;
+    const double pobj = offset + col_pobj;
+    const double dobj = (offset + row_dobj) + col_dobj;
+    const double gap = fabs(pobj - dobj) / (1.0 + fabs(pobj) + fabs(dobj));
+    const double score = maxv(maxv(primal, dual), gap);
+    st->primal_infeas = primal;
+    st->dual_infeas = dual;
+    st->gap = gap;
+    st->objective = pobj;
+    st->dual_objective = dobj;
+    st->score = score;
+    st->restart_pending = 0;
+    const long long iter = st->iter + span;
+    const long long isr = st->iters_since_restart + span;
+    int restarted = 0;
+    if (bad_rows + bad_cols > 0.0 || !isfinite(score)) {
+        // non-finite iterates: numerical_failure (the reference would run on to
+        // its iteration limit on NaNs; stopping is the engine's extension)
+        st->nonfinite = 1;
+        st->done = 1;
+        st->status = 3;
+    } else if (!final_pass && primal <= ctl.primal_tol && dual <= ctl.dual_tol && gap <= ctl.gap_tol) {
+        st->done = 1;
+        st->status = 0;
+    } else if (!final_pass) {
+        const bool do_restart =
+            ctl.strategy == 2 ||
+            (ctl.strategy == 1 && (score <= ctl.restart_reduction * st->last_restart_score ||
+                                   (isr >= 5 * ctl.restart_every && score < st->last_restart_score)));
+        if (do_restart) {
+            if (ctl.adaptive_weight && primal > 1e-12 && dual > 1e-12) {
+                const double ratio = clampv(sqrt(primal / dual), 0.05, 20.0);
+                st->omega = clampv(st->omega * pow(ratio, ctl.weight_smoothing), 1e-6, 1e6);
+            }
+            st->restart_pending = 1;
+            st->avg_count = 0;
+            st->iters_since_restart = 0;
+            st->last_restart_score = score;
+            st->restarts += 1;
+            restarted = 1;
+        } else {
+            st->avg_count += span;
+            st->iters_since_restart = isr;
+        }
+    }
+    st->iter = iter;
+    if (tr.capacity > 0 && st->checks < tr.capacity && !final_pass) {
+        const long long q = st->checks;
+        tr.iteration[q] = iter;
+        tr.primal[q] = primal;
+        tr.dual[q] = dual;
+        tr.gap[q] = gap;
+        tr.eta[q] = st->eta;
+        tr.omega[q] = st->omega;
+        tr.restarted[q] = restarted;
+    }
+    if (!final_pass) st->checks += 1;
+}
+
+// Restart to the average (pdlp.cpp:257-258): x <- x_avg, y <- y_avg.
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_restart_copy(Iterates<T> P) {
+    const DevState* st = P.st;
+    if (!st->restart_pending || st->done) return;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < P.n + P.m; t += gridDim.x * blockDim.x) {
+        if (t < P.n) P.x[t] = P.x_avg[t];
+        else P.y[t - P.n] = P.y_avg[t - P.n];
+    }
+}
+
+}  // namespace mc

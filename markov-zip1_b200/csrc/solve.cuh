@@ -1,0 +1,614 @@
+// The FP64 solve driver (included once, by engine.cu).
+#pragma once
+
+#include "engine.hpp"
+#include "iter_kernels.cuh"
+#include "setup_kernels.cuh"
+
+#include <cmath>
+#include <cstring>
+
+namespace mc {
+
+#define MC_DISPATCH_G(g, ...)                        \
+    switch (g) {                                     \
+        case 1: { constexpr int G = 1; __VA_ARGS__; } break;   \
+        case 2: { constexpr int G = 2; __VA_ARGS__; } break;   \
+        case 4: { constexpr int G = 4; __VA_ARGS__; } break;   \
+        case 8: { constexpr int G = 8; __VA_ARGS__; } break;   \
+        case 16: { constexpr int G = 16; __VA_ARGS__; } break; \
+        default: { constexpr int G = 32; __VA_ARGS__; } break; \
+    }
+
+// Launch geometry of one problem: lanes per column/row and grid sizes.
+struct Plan {
+    int g_col = 1, g_row = 1;
+    int nb_col = 1, nb_row = 1;  // SpMV kernels over columns / rows
+    int nb_m = 1, nb_nm = 1;     // elementwise kernels over m / n+m
+};
+
+Plan make_plan(const Ctx& ctx, int m, int n, long long nnz) {
+    Plan p;
+    p.g_col = pick_lanes(n > 0 ? (double)nnz / n : 1.0);
+    p.g_row = pick_lanes(m > 0 ? (double)nnz / m : 1.0);
+    p.nb_col = blocks_for(ctx, n, kBlock / p.g_col);
+    p.nb_row = blocks_for(ctx, m, kBlock / p.g_row);
+    p.nb_m = blocks_for(ctx, m, kBlock);
+    p.nb_nm = blocks_for(ctx, (long long)n + m, kBlock);
+    return p;
+}
+
+// ------------------------------------------------------------- transpose
+// CSR(A) from CSC(A): count, scan, scatter, per-row sort (ascending column,
+// so the layout and every SpMV over it are run-to-run deterministic).
+int build_csr(Ctx& ctx, int m, int n, long long nnz, const int* csc_start, const int* csc_row,
+              const double* csc_val, int* csr_start, int* csr_col, double* csr_val, int* cursor,
+              int* long_rows, int* counters /*[2]*/, int* scan_tmp) {
+    cudaStream_t s = ctx.stream;
+    CU(cudaMemsetAsync(csr_start, 0, sizeof(int) * (size_t)(m + 1), s));
+    CU(cudaMemsetAsync(cursor, 0, sizeof(int) * (size_t)m, s));
+    CU(cudaMemsetAsync(counters, 0, sizeof(int) * 2, s));
+    if (nnz > 0) {
+        ctx.begin_launch(MC_KERNEL_SETUP);
+        k_count_rows<<<blocks_for(ctx, nnz, kBlock) * 4, kBlock, 0, s>>>(nnz, csc_row, csr_start);
+        ctx.end_launch();
+    }
+    // inclusive scan of the m+1 counts, multi-level over tile totals
+    std::vector<std::pair<int*, long long>> levels;
+    {
+        int* data = csr_start;
+        long long len = m + 1;
+        int* tmp = scan_tmp;
+        while (true) {
+            const long long tiles = (len + kScanTile - 1) / kScanTile;
+            ctx.begin_launch(MC_KERNEL_SETUP);
+            k_scan_tiles<<<(unsigned)tiles, kScanThreads, 0, s>>>(data, len, tmp);
+            ctx.end_launch();
+            levels.push_back({data, len});
+            if (tiles == 1) break;
+            data = tmp;
+            len = tiles;
+            tmp += (tiles + 255) & ~255LL;
+        }
+        for (int l = (int)levels.size() - 2; l >= 0; --l) {
+            const long long tiles = (levels[l].second + kScanTile - 1) / kScanTile;
+            ctx.begin_launch(MC_KERNEL_SETUP);
+            k_scan_add<<<(unsigned)tiles, kBlock, 0, s>>>(levels[l].first, levels[l].second, levels[l + 1].first);
+            ctx.end_launch();
+        }
+    }
+    if (nnz == 0) return ctx.launch_check("build_csr");
+    const int nb_n = (int)((n + kBlock - 1) / kBlock);
+    const int nb_m = (int)((m + kBlock - 1) / kBlock);
+    ctx.begin_launch(MC_KERNEL_SETUP);
+    k_scatter_rows<<<nb_n, kBlock, 0, s>>>(n, csc_start, csc_row, csc_val, csr_start, cursor, csr_col, csr_val);
+    ctx.end_launch();
+    ctx.begin_launch(MC_KERNEL_SETUP);
+    k_sort_short_rows<<<nb_m, kBlock, 0, s>>>(m, csr_start, csr_col, csr_val, long_rows, counters);
+    ctx.end_launch();
+    ctx.begin_launch(MC_KERNEL_SETUP);
+    k_max_line<<<blocks_for(ctx, m, kBlock), kBlock, 0, s>>>(m, csr_start, counters + 1);
+    ctx.end_launch();
+    int host_counters[2] = {0, 0};
+    CU(cudaMemcpyAsync(host_counters, counters, sizeof host_counters, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    TRY(ctx.drain_profile());
+    if (host_counters[0] > 0) {
+        int* tmp_col = nullptr;
+        double* tmp_val = nullptr;
+        if (host_counters[1] > kSmemSortRow) {
+            CU(cudaMallocAsync(reinterpret_cast<void**>(&tmp_col), sizeof(int) * (size_t)nnz, s));
+            CU(cudaMallocAsync(reinterpret_cast<void**>(&tmp_val), sizeof(double) * (size_t)nnz, s));
+        }
+        const size_t smem = (size_t)kSmemSortRow * (sizeof(int) + sizeof(double));
+        ctx.begin_launch(MC_KERNEL_SETUP);
+        k_sort_long_rows<<<host_counters[0], 1024, smem, s>>>(long_rows, csr_start, csr_col, csr_val, tmp_col, tmp_val);
+        ctx.end_launch();
+        if (tmp_col) {
+            CU(cudaFreeAsync(tmp_col, s));
+            CU(cudaFreeAsync(tmp_val, s));
+        }
+    }
+    return ctx.launch_check("build_csr");
+}
+
+// ------------------------------------------------------------------ Ruiz
+int ruiz(Ctx& ctx, int m, int n, long long nnz, const int* csc_start, const int* csc_row, double* csc_val,
+         const int* csr_start, const int* csr_col, double* csr_val, double* row_scale, double* col_scale,
+         double* r_tmp, double* c_tmp, double* partials, DevState* st, long long passes) {
+    cudaStream_t s = ctx.stream;
+    ctx.begin_launch(MC_KERNEL_SETUP);
+    k_fill<double><<<blocks_for(ctx, m, kBlock), kBlock, 0, s>>>(row_scale, m, 1.0);
+    ctx.end_launch();
+    ctx.begin_launch(MC_KERNEL_SETUP);
+    k_fill<double><<<blocks_for(ctx, n, kBlock), kBlock, 0, s>>>(col_scale, n, 1.0);
+    ctx.end_launch();
+    if (nnz == 0) return ctx.launch_check("ruiz");
+    const int nbc = blocks_for(ctx, n, kBlock), nbr = blocks_for(ctx, m, kBlock);
+    for (long long pass = 0; pass < passes; ++pass) {
+        ctx.begin_launch(MC_KERNEL_SETUP);
+        k_ruiz_line_max<<<nbc, kBlock, 0, s>>>(n, csc_start, csc_val, c_tmp, partials + SLOT_A * kMaxPartials, st);
+        ctx.end_launch();
+        ctx.begin_launch(MC_KERNEL_SETUP);
+        k_ruiz_line_max<<<nbr, kBlock, 0, s>>>(m, csr_start, csr_val, r_tmp, partials + SLOT_B * kMaxPartials, st);
+        ctx.end_launch();
+        ctx.begin_launch(MC_KERNEL_SETUP);
+        k_ruiz_check<<<1, 1024, 0, s>>>(partials + SLOT_B * kMaxPartials, nbr, partials + SLOT_A * kMaxPartials,
+                                        nbc, 1e-3, st);
+        ctx.end_launch();
+        ctx.begin_launch(MC_KERNEL_SETUP);
+        k_ruiz_deltas<<<nbr, kBlock, 0, s>>>(m, r_tmp, row_scale, st);
+        ctx.end_launch();
+        ctx.begin_launch(MC_KERNEL_SETUP);
+        k_ruiz_deltas<<<nbc, kBlock, 0, s>>>(n, c_tmp, col_scale, st);
+        ctx.end_launch();
+        ctx.begin_launch(MC_KERNEL_SETUP);
+        k_ruiz_rescale<<<nbc, kBlock, 0, s>>>(n, csc_start, csc_row, csc_val, c_tmp, r_tmp, 0, st);
+        ctx.end_launch();
+        ctx.begin_launch(MC_KERNEL_SETUP);
+        k_ruiz_rescale<<<nbr, kBlock, 0, s>>>(m, csr_start, csr_col, csr_val, r_tmp, c_tmp, 1, st);
+        ctx.end_launch();
+    }
+    return ctx.launch_check("ruiz");
+}
+
+// ------------------------------------------------------- iteration chunks
+template <class T>
+int enqueue_iteration(Ctx& ctx, const Iterates<T>& P, const Plan& pl, int k, bool step, const Controls& ctl) {
+    cudaStream_t s = ctx.stream;
+    ctx.begin_launch(MC_KERNEL_PRIMAL);
+    if (step) {
+        MC_DISPATCH_G(pl.g_col, (k_primal<G, true, T><<<pl.nb_col, kBlock, 0, s>>>(P, k)));
+    } else {
+        MC_DISPATCH_G(pl.g_col, (k_primal<G, false, T><<<pl.nb_col, kBlock, 0, s>>>(P, k)));
+    }
+    ctx.end_launch();
+    if (step) {
+        ctx.begin_launch(MC_KERNEL_DUAL_STEP);
+        MC_DISPATCH_G(pl.g_row, (k_dual_probe<G, T><<<pl.nb_row, kBlock, 0, s>>>(P)));
+        ctx.end_launch();
+        ctx.begin_launch(MC_KERNEL_OTHER);
+        k_step_size<<<1, 1024, 0, s>>>(P.partials, pl.nb_col, pl.nb_row, P.st, ctl);
+        ctx.end_launch();
+        ctx.begin_launch(MC_KERNEL_DUAL_STEP);
+        k_dual_apply<T><<<pl.nb_m, kBlock, 0, s>>>(P, k);
+        ctx.end_launch();
+    } else {
+        ctx.begin_launch(MC_KERNEL_DUAL);
+        MC_DISPATCH_G(pl.g_row, (k_dual<G, T><<<pl.nb_row, kBlock, 0, s>>>(P, k)));
+        ctx.end_launch();
+    }
+    return ctx.launch_check("iteration");
+}
+
+template <class T>
+int enqueue_check(Ctx& ctx, const Iterates<T>& P, const Original& O, const Plan& pl, long long span,
+                  int final_pass, const Controls& ctl, const TraceBuf& tr) {
+    cudaStream_t s = ctx.stream;
+    ctx.begin_launch(MC_KERNEL_RESIDUAL);
+    MC_DISPATCH_G(pl.g_row, (k_residual_rows<G, T><<<pl.nb_row, kBlock, 0, s>>>(P, O)));
+    ctx.end_launch();
+    ctx.begin_launch(MC_KERNEL_RESIDUAL);
+    MC_DISPATCH_G(pl.g_col, (k_residual_cols<G, T><<<pl.nb_col, kBlock, 0, s>>>(P, O)));
+    ctx.end_launch();
+    ctx.begin_launch(MC_KERNEL_RESIDUAL);
+    k_finalize<<<1, 1024, 0, s>>>(P.partials, pl.nb_row, pl.nb_col, span, final_pass, O.offset, ctl, tr, P.st);
+    ctx.end_launch();
+    if (!final_pass) {
+        ctx.begin_launch(MC_KERNEL_OTHER);
+        k_restart_copy<T><<<pl.nb_nm, kBlock, 0, s>>>(P);
+        ctx.end_launch();
+    }
+    return ctx.launch_check("check");
+}
+
+// iterations [k0, k1) of the chunk that starts at global iteration `base`
+template <class T>
+int enqueue_span(Ctx& ctx, const Iterates<T>& P, const Plan& pl, long long base, int k0, int k1,
+                 const Controls& ctl) {
+    for (int k = k0; k < k1; ++k) {
+        const bool step = ctl.adaptive_step && ((base + k) % 10 == 0);
+        TRY(enqueue_iteration(ctx, P, pl, k, step, ctl));
+    }
+    return MC_OK;
+}
+
+// Capture one full chunk (restart_every iterations + check) as a graph; the
+// schedule of step-size iterations depends only on base % 10.
+template <class T>
+int chunk_graph(Ctx& ctx, const Iterates<T>& P, const Original& O, const Plan& pl, long long base,
+                long long R, const Controls& ctl, const TraceBuf& tr, cudaGraphExec_t* out,
+                long long recipe[MC_KERNEL_KINDS]) {
+    const int key = (int)(base % 10);
+    long long before[MC_KERNEL_KINDS];
+    std::memcpy(before, ctx.launches, sizeof before);
+    CU(cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeThreadLocal));
+    ctx.capturing = true;
+    int rc = enqueue_span(ctx, P, pl, base, 0, (int)R, ctl);
+    if (rc == MC_OK) rc = enqueue_check(ctx, P, O, pl, R, 0, ctl, tr);
+    ctx.capturing = false;
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(ctx.stream, &g);
+    for (int q = 0; q < MC_KERNEL_KINDS; ++q) {
+        recipe[q] = ctx.launches[q] - before[q];
+        ctx.launches[q] = before[q];
+    }
+    if (rc != MC_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture", __LINE__);
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t e2 = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e2 != cudaSuccess) return cuda_fail(e2, "cudaGraphInstantiate", __LINE__);
+    ctx.graphs[key] = exec;
+    *out = exec;
+    return MC_OK;
+}
+
+// ------------------------------------------------------------------ solve
+static void fill_message(mc_pdlp_result* r, const char* msg) {
+    std::snprintf(r->message, sizeof r->message, "%s", msg);
+}
+
+int validate_options(const mc_pdlp_options* o) {
+    if (!o) return set_error(MC_ERR_INVALID_ARGUMENT, "options is NULL");
+    if (o->backend != MC_BACKEND_GPU)
+        return set_error(MC_ERR_INVALID_ARGUMENT,
+                         "backend must be MC_BACKEND_GPU: this engine has no CPU path");
+    if (o->restart_every <= 0) return set_error(MC_ERR_INVALID_ARGUMENT, "restart_every must be positive");
+    if (o->max_iterations < 0) return set_error(MC_ERR_INVALID_ARGUMENT, "max_iterations must be >= 0");
+    if (o->restart_every > (1 << 20))
+        return set_error(MC_ERR_INVALID_ARGUMENT, "restart_every above 2^20 is not supported");
+    if (o->ruiz_iterations < 0) return set_error(MC_ERR_INVALID_ARGUMENT, "ruiz_iterations must be >= 0");
+    if (!(o->restart_strategy >= 0 && o->restart_strategy <= 2))
+        return set_error(MC_ERR_INVALID_ARGUMENT, "unknown restart_strategy %d", o->restart_strategy);
+    if (o->precision != MC_PRECISION_FP64 && o->precision != MC_PRECISION_FP32_REFINE)
+        return set_error(MC_ERR_INVALID_ARGUMENT, "unknown precision %d", o->precision);
+    return MC_OK;
+}
+
+int validate_lp(const mc_lp* lp) {
+    if (!lp) return set_error(MC_ERR_INVALID_ARGUMENT, "lp is NULL");
+    if (lp->num_rows < 0 || lp->num_cols < 0 || lp->nnz < 0)
+        return set_error(MC_ERR_INVALID_ARGUMENT, "negative dimension");
+    if (lp->nnz >= (1LL << 31) - 1)
+        return set_error(MC_ERR_RESOURCE_LIMIT, "nnz %lld exceeds the int32 index range", (long long)lp->nnz);
+    if (lp->memory != MC_MEMORY_HOST && lp->memory != MC_MEMORY_DEVICE)
+        return set_error(MC_ERR_INVALID_ARGUMENT, "unknown memory kind %d", lp->memory);
+    if (lp->num_rows == 0 || lp->num_cols == 0) return MC_OK;
+    if (!lp->col_start || (lp->nnz > 0 && (!lp->row_index || !lp->value)) || !lp->objective ||
+        !lp->var_lower || !lp->var_upper || !lp->row_lower || !lp->row_upper)
+        return set_error(MC_ERR_INVALID_ARGUMENT, "NULL array in lp");
+    if (lp->memory == MC_MEMORY_HOST) {
+        // cheap host checks first: the device validation re-checks everything
+        if (lp->col_start[0] != 0 || (long long)lp->col_start[lp->num_cols] != lp->nnz)
+            return set_error(MC_ERR_INVALID_ARGUMENT, "CSC terminal pointer mismatch");
+    }
+    return MC_OK;
+}
+
+int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* warm_x,
+             const double* warm_y, double* x_out, double* y_out, mc_pdlp_result* res,
+             mc_pdlp_trace* trace) {
+    const double t_begin = now_ms();
+    if (!res) return set_error(MC_ERR_INVALID_ARGUMENT, "result is NULL");
+    std::memset(res, 0, sizeof *res);
+    std::snprintf(res->backend_actually_used, sizeof res->backend_actually_used, "cuda");
+    if (trace) trace->count = 0;
+    TRY(validate_options(o));
+    TRY(validate_lp(lp));
+    if (o->precision == MC_PRECISION_FP32_REFINE) return solve_fp32_refine(ctx, lp, o, warm_x, warm_y, x_out, y_out, res, trace);
+    const int m = lp->num_rows, n = lp->num_cols;
+    const long long nnz = lp->nnz;
+    if (m == 0 || n == 0) {  // pdlp.cpp:144-149
+        res->status = MC_PDLP_OPTIMAL;
+        res->tolerance = o->primal_tolerance;
+        fill_message(res, "trivial");
+        res->total_ms = now_ms() - t_begin;
+        return MC_OK;
+    }
+    const bool dev_in = lp->memory == MC_MEMORY_DEVICE;
+    cudaStream_t s = ctx.stream;
+    for (int q = 0; q < MC_KERNEL_KINDS; ++q) {
+        ctx.launches[q] = 0;
+        ctx.kernel_ms[q] = 0.0;
+    }
+    ctx.profiling = o->profile_kernels != 0;
+    ctx.pending.clear();
+    ctx.prof_used = 0;
+    ctx.release_graphs();
+
+    // ---- arena layout
+    const long long trace_cap = trace ? trace->capacity : 0;
+    Layout L;
+    const size_t o_csc_start = dev_in ? 0 : L.add<int>(n + 1);
+    const size_t o_csc_row = dev_in ? 0 : L.add<int>(nnz);
+    const size_t o_csc_val = L.add<double>(nnz);
+    const size_t o_csr_start = L.add<int>(m + 1);
+    const size_t o_csr_col = L.add<int>(nnz);
+    const size_t o_csr_val = L.add<double>(nnz);
+    const size_t o_cursor = L.add<int>(m);
+    const size_t o_long = L.add<int>(m);
+    const size_t o_counters = L.add<int>(4);
+    const size_t o_scan = L.add<int>((m + 1) / kScanTile + 4096);
+    const size_t o_in_obj = dev_in ? 0 : L.add<double>(n);
+    const size_t o_in_lo = dev_in ? 0 : L.add<double>(n);
+    const size_t o_in_hi = dev_in ? 0 : L.add<double>(n);
+    const size_t o_in_rlo = dev_in ? 0 : L.add<double>(m);
+    const size_t o_in_rhi = dev_in ? 0 : L.add<double>(m);
+    const size_t o_warm_x = (!dev_in && warm_x) ? L.add<double>(n) : 0;
+    const size_t o_warm_y = (!dev_in && warm_y) ? L.add<double>(m) : 0;
+    size_t o_n[14], o_m[12];
+    for (auto& v : o_n) v = L.add<double>(n);
+    for (auto& v : o_m) v = L.add<double>(m);
+    const size_t o_partials = L.add<double>((long long)NUM_SLOTS * kMaxPartials);
+    const size_t o_state = L.add<DevState>(1);
+    const size_t o_tr_it = L.add<long long>(trace_cap);
+    size_t o_tr[5];
+    for (auto& v : o_tr) v = L.add<double>(trace_cap);
+    const size_t o_tr_rs = L.add<int>(trace_cap);
+    TRY(ctx.arena.reserve(L.offset));
+    char* A = static_cast<char*>(ctx.arena.base);
+    auto at = [&](size_t off) { return static_cast<void*>(A + off); };
+
+    const int* csc_start = dev_in ? lp->col_start : static_cast<int*>(at(o_csc_start));
+    const int* csc_row = dev_in ? lp->row_index : static_cast<int*>(at(o_csc_row));
+    double* csc_val = static_cast<double*>(at(o_csc_val));
+    int* csr_start = static_cast<int*>(at(o_csr_start));
+    int* csr_col = static_cast<int*>(at(o_csr_col));
+    double* csr_val = static_cast<double*>(at(o_csr_val));
+    const double* in_obj = dev_in ? lp->objective : static_cast<double*>(at(o_in_obj));
+    const double* in_lo = dev_in ? lp->var_lower : static_cast<double*>(at(o_in_lo));
+    const double* in_hi = dev_in ? lp->var_upper : static_cast<double*>(at(o_in_hi));
+    const double* in_rlo = dev_in ? lp->row_lower : static_cast<double*>(at(o_in_rlo));
+    const double* in_rhi = dev_in ? lp->row_upper : static_cast<double*>(at(o_in_rhi));
+    const double* d_warm_x = warm_x ? (dev_in ? warm_x : static_cast<double*>(at(o_warm_x))) : nullptr;
+    const double* d_warm_y = warm_y ? (dev_in ? warm_y : static_cast<double*>(at(o_warm_y))) : nullptr;
+    double* c = static_cast<double*>(at(o_n[0]));
+    double* lo = static_cast<double*>(at(o_n[1]));
+    double* hi = static_cast<double*>(at(o_n[2]));
+    double* c_orig = static_cast<double*>(at(o_n[3]));
+    double* lo_orig = static_cast<double*>(at(o_n[4]));
+    double* hi_orig = static_cast<double*>(at(o_n[5]));
+    double* col_norm = static_cast<double*>(at(o_n[6]));
+    double* col_scale = static_cast<double*>(at(o_n[7]));
+    double* x = static_cast<double*>(at(o_n[8]));
+    double* x_bar = static_cast<double*>(at(o_n[9]));
+    double* x_avg = static_cast<double*>(at(o_n[10]));
+    double* dx = static_cast<double*>(at(o_n[11]));
+    double* x_stage = static_cast<double*>(at(o_n[12]));
+    double* blo = static_cast<double*>(at(o_m[0]));
+    double* bhi = static_cast<double*>(at(o_m[1]));
+    double* blo_orig = static_cast<double*>(at(o_m[2]));
+    double* bhi_orig = static_cast<double*>(at(o_m[3]));
+    double* row_norm = static_cast<double*>(at(o_m[4]));
+    double* row_scale = static_cast<double*>(at(o_m[5]));
+    double* y = static_cast<double*>(at(o_m[6]));
+    double* y_avg = static_cast<double*>(at(o_m[7]));
+    double* ax_bar = static_cast<double*>(at(o_m[8]));
+    double* y_stage = static_cast<double*>(at(o_m[9]));
+    double* partials = static_cast<double*>(at(o_partials));
+    DevState* st = static_cast<DevState*>(at(o_state));
+
+    // ---- uploads
+    CU(cudaEventRecord(ctx.ev_a, s));
+    const cudaMemcpyKind in_kind = dev_in ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    if (!dev_in) {
+        CU(cudaMemcpyAsync(at(o_csc_start), lp->col_start, sizeof(int) * (size_t)(n + 1), in_kind, s));
+        if (nnz) CU(cudaMemcpyAsync(at(o_csc_row), lp->row_index, sizeof(int) * (size_t)nnz, in_kind, s));
+        CU(cudaMemcpyAsync(at(o_in_obj), lp->objective, sizeof(double) * (size_t)n, in_kind, s));
+        CU(cudaMemcpyAsync(at(o_in_lo), lp->var_lower, sizeof(double) * (size_t)n, in_kind, s));
+        CU(cudaMemcpyAsync(at(o_in_hi), lp->var_upper, sizeof(double) * (size_t)n, in_kind, s));
+        CU(cudaMemcpyAsync(at(o_in_rlo), lp->row_lower, sizeof(double) * (size_t)m, in_kind, s));
+        CU(cudaMemcpyAsync(at(o_in_rhi), lp->row_upper, sizeof(double) * (size_t)m, in_kind, s));
+        if (warm_x) CU(cudaMemcpyAsync(at(o_warm_x), warm_x, sizeof(double) * (size_t)n, in_kind, s));
+        if (warm_y) CU(cudaMemcpyAsync(at(o_warm_y), warm_y, sizeof(double) * (size_t)m, in_kind, s));
+    }
+    if (nnz) CU(cudaMemcpyAsync(csc_val, lp->value, sizeof(double) * (size_t)nnz, in_kind, s));
+    CU(cudaEventRecord(ctx.ev_b, s));
+
+    // ---- validation (every later gather depends on it)
+    int* counters = static_cast<int*>(at(o_counters));
+    CU(cudaMemsetAsync(counters, 0, sizeof(int) * 4, s));
+    ctx.begin_launch(MC_KERNEL_SETUP);
+    k_validate_csc<<<(n + kBlock - 1) / kBlock, kBlock, 0, s>>>(m, n, nnz, csc_start, csc_row, csc_val, counters + 2);
+    ctx.end_launch();
+    int bad = 0;
+    CU(cudaMemcpyAsync(&bad, counters + 2, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    TRY(ctx.drain_profile());
+    if (bad) {
+        return set_error(MC_ERR_INVALID_ARGUMENT, "invalid CSC matrix (%s%s%s%s)",
+                         (bad & 1) ? "column pointers " : "", (bad & 2) ? "row index out of range " : "",
+                         (bad & 4) ? "rows not strictly increasing " : "",
+                         (bad & 8) ? "zero or non-finite value" : "");
+    }
+
+    // ---- setup
+    CU(cudaMemsetAsync(st, 0, sizeof(DevState), s));
+    TRY(build_csr(ctx, m, n, nnz, csc_start, csc_row, csc_val, csr_start, csr_col, csr_val,
+                  static_cast<int*>(at(o_cursor)), static_cast<int*>(at(o_long)), counters,
+                  static_cast<int*>(at(o_scan))));
+    TRY(ruiz(ctx, m, n, nnz, csc_start, csc_row, csc_val, csr_start, csr_col, csr_val, row_scale, col_scale,
+             ax_bar, dx, partials, st, o->ruiz_scaling ? o->ruiz_iterations : 0));
+    const double obj_sign = (lp->objective_sense == MC_MAXIMIZE) ? -1.0 : 1.0;
+    const int nbc = blocks_for(ctx, n, kBlock), nbr = blocks_for(ctx, m, kBlock);
+    ctx.begin_launch(MC_KERNEL_SETUP);
+    k_setup_cols<<<nbc, kBlock, 0, s>>>(n, csc_start, csc_val, in_obj, in_lo, in_hi, col_scale, d_warm_x, obj_sign,
+                                        c, lo, hi, c_orig, lo_orig, hi_orig, col_norm, x, x_avg, partials);
+    ctx.end_launch();
+    ctx.begin_launch(MC_KERNEL_SETUP);
+    k_setup_rows<<<nbr, kBlock, 0, s>>>(m, csr_start, csr_val, in_rlo, in_rhi, row_scale, d_warm_y, blo, bhi,
+                                        blo_orig, bhi_orig, row_norm, y, y_avg, partials);
+    ctx.end_launch();
+    ctx.begin_launch(MC_KERNEL_SETUP);
+    k_setup_scalars<<<1, 1024, 0, s>>>(partials, nbc, nbr, o->initial_primal_weight, o->step_size_reduction, st);
+    ctx.end_launch();
+    TRY(ctx.launch_check("setup"));
+
+    Iterates<double> P;
+    P.m = m;
+    P.n = n;
+    P.csc_start = csc_start;
+    P.csc_row = csc_row;
+    P.csc_val = csc_val;
+    P.csr_start = csr_start;
+    P.csr_col = csr_col;
+    P.csr_val = csr_val;
+    P.c = c;
+    P.lo = lo;
+    P.hi = hi;
+    P.blo = blo;
+    P.bhi = bhi;
+    P.col_norm = col_norm;
+    P.row_norm = row_norm;
+    P.x = x;
+    P.x_bar = x_bar;
+    P.x_avg = x_avg;
+    P.dx = dx;
+    P.y = y;
+    P.y_avg = y_avg;
+    P.ax_bar = ax_bar;
+    P.partials = partials;
+    P.st = st;
+    Original O{c_orig, in_obj, lo_orig, hi_orig, blo_orig, bhi_orig, col_scale, row_scale, lp->objective_offset};
+    Controls ctl{o->primal_tolerance, o->dual_tolerance, o->gap_tolerance, o->restart_reduction_factor,
+                 o->primal_weight_smoothing, o->restart_every, o->restart_strategy, o->adaptive_step_size,
+                 o->adaptive_primal_weight};
+    TraceBuf tr{trace_cap, static_cast<long long*>(at(o_tr_it)), static_cast<double*>(at(o_tr[0])),
+                static_cast<double*>(at(o_tr[1])), static_cast<double*>(at(o_tr[2])),
+                static_cast<double*>(at(o_tr[3])), static_cast<double*>(at(o_tr[4])),
+                static_cast<int*>(at(o_tr_rs))};
+    const Plan pl = make_plan(ctx, m, n, nnz);
+
+    // ---- PDHG loop in restart chunks
+    const long long R = o->restart_every;
+    const long long maxit = o->max_iterations;
+    const long long full_chunks = maxit / R;
+    const int poll_every = o->check_every_chunks > 0 ? o->check_every_chunks : 1;
+    long long base = 0;
+    bool done = false;
+    long long recipe[10][MC_KERNEL_KINDS] = {};
+    int inflight = 0;  // chunks launched since the last poll-able event
+    long long polled_chunks = 0;
+    int ev_idx = 0;
+    bool have_prev = false;
+    for (long long chunk = 0; chunk < full_chunks && !done; ++chunk) {
+        if (ctx.profiling) {
+            TRY(enqueue_span(ctx, P, pl, base, 0, (int)R, ctl));
+            TRY(enqueue_check(ctx, P, O, pl, R, 0, ctl, tr));
+            TRY(ctx.drain_profile());
+        } else {
+            const int key = (int)(base % 10);
+            auto it = ctx.graphs.find(key);
+            cudaGraphExec_t exec = nullptr;
+            if (it == ctx.graphs.end()) {
+                TRY(chunk_graph(ctx, P, O, pl, base, R, ctl, tr, &exec, recipe[key]));
+            } else {
+                exec = it->second;
+            }
+            CU(cudaGraphLaunch(exec, s));
+            for (int q = 0; q < MC_KERNEL_KINDS; ++q) ctx.launches[q] += recipe[key][q];
+        }
+        base += R;
+        ++inflight;
+        if (inflight >= poll_every || chunk + 1 == full_chunks) {
+            // poll the previous event (one chunk group behind), then record a new one
+            if (have_prev) {
+                CU(cudaEventSynchronize(ctx.ev_poll[ev_idx ^ 1]));
+                if (ctx.h_state[ev_idx ^ 1].done) done = true;
+            }
+            CU(cudaMemcpyAsync(&ctx.h_state[ev_idx], st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
+            CU(cudaEventRecord(ctx.ev_poll[ev_idx], s));
+            have_prev = true;
+            ev_idx ^= 1;
+            inflight = 0;
+            ++polled_chunks;
+        }
+    }
+    CU(cudaStreamSynchronize(s));
+    CU(cudaMemcpy(&ctx.h_state[2], st, sizeof(DevState), cudaMemcpyDeviceToHost));
+    done = ctx.h_state[2].done != 0;
+    if (!done) {
+        // the loop ran out: remaining partial chunk, then the final evaluation
+        // (pdlp.cpp:263-265); after a whole number of chunks the last check
+        // already holds the averages' residuals
+        const long long rem = maxit - full_chunks * R;
+        if (rem > 0 || full_chunks == 0) {
+            TRY(enqueue_span(ctx, P, pl, base, 0, (int)rem, ctl));
+            TRY(enqueue_check(ctx, P, O, pl, rem, 1, ctl, tr));
+            TRY(ctx.drain_profile());
+        }
+    }
+    CU(cudaEventRecord(ctx.ev_c, s));
+
+    // ---- outputs
+    const bool dev_out = dev_in;
+    double* xo = dev_out ? x_out : (x_out ? x_stage : nullptr);
+    double* yo = dev_out ? y_out : (y_out ? y_stage : nullptr);
+    if (xo || yo) {
+        ctx.begin_launch(MC_KERNEL_OTHER);
+        k_unscale_out<<<pl.nb_nm, kBlock, 0, s>>>(n, m, x_avg, y_avg, col_scale, row_scale, xo, yo);
+        ctx.end_launch();
+        TRY(ctx.launch_check("unscale"));
+    }
+    cudaEvent_t ev_d2h = ctx.ev_d;
+    CU(cudaEventRecord(ctx.ev_c, s));
+    if (!dev_out) {
+        if (x_out) CU(cudaMemcpyAsync(x_out, x_stage, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, s));
+        if (y_out) CU(cudaMemcpyAsync(y_out, y_stage, sizeof(double) * (size_t)m, cudaMemcpyDeviceToHost, s));
+    }
+    CU(cudaMemcpyAsync(&ctx.h_state[3], st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
+    CU(cudaEventRecord(ev_d2h, s));
+    CU(cudaStreamSynchronize(s));
+    TRY(ctx.drain_profile());
+    const DevState& S = ctx.h_state[3];
+    if (trace && trace_cap > 0) {
+        const long long cnt = std::min<long long>(S.checks, trace_cap);
+        trace->count = cnt;
+        if (cnt > 0) {
+            CU(cudaMemcpy(trace->iteration, at(o_tr_it), sizeof(long long) * cnt, cudaMemcpyDeviceToHost));
+            CU(cudaMemcpy(trace->primal_infeasibility, at(o_tr[0]), sizeof(double) * cnt, cudaMemcpyDeviceToHost));
+            CU(cudaMemcpy(trace->dual_infeasibility, at(o_tr[1]), sizeof(double) * cnt, cudaMemcpyDeviceToHost));
+            CU(cudaMemcpy(trace->duality_gap, at(o_tr[2]), sizeof(double) * cnt, cudaMemcpyDeviceToHost));
+            CU(cudaMemcpy(trace->step_size, at(o_tr[3]), sizeof(double) * cnt, cudaMemcpyDeviceToHost));
+            CU(cudaMemcpy(trace->primal_weight, at(o_tr[4]), sizeof(double) * cnt, cudaMemcpyDeviceToHost));
+            CU(cudaMemcpy(trace->restarted, at(o_tr_rs), sizeof(int) * cnt, cudaMemcpyDeviceToHost));
+        }
+    }
+    float h2d = 0.f, kern = 0.f, d2h = 0.f;
+    CU(cudaEventElapsedTime(&h2d, ctx.ev_a, ctx.ev_b));
+    CU(cudaEventElapsedTime(&kern, ctx.ev_b, ctx.ev_c));
+    CU(cudaEventElapsedTime(&d2h, ctx.ev_c, ev_d2h));
+    res->status = S.status;
+    res->objective = S.objective;
+    res->primal_infeasibility = S.primal_infeas;
+    res->dual_infeasibility = S.dual_infeas;
+    res->duality_gap = S.gap;
+    res->tolerance = o->primal_tolerance;
+    res->iterations = S.iter;
+    fill_message(res, S.status == MC_PDLP_OPTIMAL ? "PDLP converged"
+                      : S.status == MC_PDLP_NUMERICAL_FAILURE ? "non-finite iterate or residual"
+                                                              : "iteration limit reached");
+    res->h2d_ms = dev_in ? 0.0 : h2d;
+    res->kernel_ms = kern + (dev_in ? h2d : 0.0);
+    res->d2h_ms = dev_out ? 0.0 : d2h;
+    res->ruiz_iterations_executed = o->ruiz_scaling ? S.ruiz_passes : 0;
+    res->restarts = S.restarts;
+    res->final_primal_weight = S.omega;
+    res->final_step_size = S.eta;
+    long long total = 0;
+    for (int q = 0; q < MC_KERNEL_KINDS; ++q) {
+        res->launches_by_kind[q] = ctx.launches[q];
+        res->kernel_ms_by_kind[q] = ctx.kernel_ms[q];
+        total += ctx.launches[q];
+    }
+    res->kernel_launches = total;
+    res->total_ms = now_ms() - t_begin;
+    (void)polled_chunks;
+    return MC_OK;
+}
+
+}  // namespace mc

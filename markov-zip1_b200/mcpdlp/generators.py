@@ -1,0 +1,103 @@
+"""Seeded synthetic LP workloads (thin wrappers over gen/lpgen.c).
+
+Families, sizes and distributions follow the engine's workloads:
+  * ``random_lp``      -- equality-row LP with analytic optimum c.x* = b.y*
+                          (k nonzeros per column, N(0,1) values, 0 <= x <= 10)
+  * ``random_lp(..., family="precision")`` -- |a| log-uniform on [1e-3, 1e3]
+                          with random sign; 20% of columns boxed by U(1,100)
+  * ``transport``      -- transportation LP (supply <=, demand =, x >= 0)
+  * ``tighten_bounds`` -- branch-and-bound style node variants of a base LP
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _lib
+from .model import Model, ObjectiveSense
+
+FAMILIES = {"standard": 0, "precision": 1}
+
+# Shapes of the named workloads.
+CONFIG0 = dict(m=1000, n=3000, k=6)               # small LP with known optimum
+CONFIG1 = dict(m=2_000_000, n=5_000_000, k=8)     # 40M nonzeros, FP64
+CONFIG2 = dict(m=1_000_000, n=3_000_000, k=10, family="precision")  # 30M nonzeros
+
+
+def _p(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def random_lp(seed: int, m: int, n: int, k: int, family: str = "standard") -> Model:
+    lib = _lib.lpgen()
+    nnz = n * k
+    col_start = np.empty(n + 1, np.int32)
+    row_index = np.empty(nnz, np.int32)
+    value = np.empty(nnz, np.float64)
+    objective = np.empty(n, np.float64)
+    var_lower = np.empty(n, np.float64)
+    var_upper = np.empty(n, np.float64)
+    row_lower = np.empty(m, np.float64)
+    row_upper = np.empty(m, np.float64)
+    x_star = np.empty(n, np.float64)
+    y_star = np.empty(m, np.float64)
+    opt = np.empty(2, np.float64)
+    rc = lib.lpgen_random_lp(seed, m, n, k, FAMILIES[family], _p(col_start), _p(row_index),
+                             _p(value), _p(objective), _p(var_lower), _p(var_upper),
+                             _p(row_lower), _p(row_upper), _p(x_star), _p(y_star), _p(opt))
+    if rc != 0:
+        raise ValueError(f"lpgen_random_lp rejected m={m} n={n} k={k} ({rc})")
+    return Model(m, n, col_start, row_index, value, objective, var_lower, var_upper,
+                 row_lower, row_upper, 0.0, ObjectiveSense.minimize,
+                 name=f"random-{family}-s{seed}-{m}x{n}k{k}",
+                 info=dict(x_star=x_star, y_star=y_star, optimum=float(opt[0]),
+                           dual_optimum=float(opt[1]), seed=seed, family=family))
+
+
+def transport(seed: int, S: int | None = None, D: int | None = None) -> Model:
+    """Transportation LP; S and D default to U[50,500] drawn from the seed."""
+    lib = _lib.lpgen()
+    if S is None:
+        S = int(lib.lpgen_uniform_int(seed, 0, 50, 500))
+    if D is None:
+        D = int(lib.lpgen_uniform_int(seed, 1, 50, 500))
+    m, n = S + D, S * D
+    col_start = np.empty(n + 1, np.int32)
+    row_index = np.empty(2 * n, np.int32)
+    value = np.empty(2 * n, np.float64)
+    objective = np.empty(n, np.float64)
+    var_lower = np.empty(n, np.float64)
+    var_upper = np.empty(n, np.float64)
+    row_lower = np.empty(m, np.float64)
+    row_upper = np.empty(m, np.float64)
+    sup = np.empty(2 * S, np.float64)
+    dem = np.empty(2 * D, np.float64)
+    rc = lib.lpgen_transport(seed, S, D, _p(col_start), _p(row_index), _p(value),
+                             _p(objective), _p(var_lower), _p(var_upper), _p(row_lower),
+                             _p(row_upper), _p(sup), _p(dem))
+    if rc != 0:
+        raise ValueError(f"lpgen_transport rejected S={S} D={D} ({rc})")
+    return Model(m, n, col_start, row_index, value, objective, var_lower, var_upper,
+                 row_lower, row_upper, 0.0, ObjectiveSense.minimize,
+                 name=f"transport-s{seed}-{S}x{D}",
+                 info=dict(S=S, D=D, supply_xy=sup.reshape(S, 2), demand_xy=dem.reshape(D, 2),
+                           seed=seed))
+
+
+def tighten_bounds(base: Model, seed: int) -> tuple[Model, np.ndarray]:
+    """A node variant of ``base``: 1-10 bounds tightened around x*."""
+    lib = _lib.lpgen()
+    x_star = base.info["x_star"]
+    lo = base.var_lower.copy()
+    hi = base.var_upper.copy()
+    cols = np.zeros(10, np.int32)
+    cnt = lib.lpgen_tighten_bounds(seed, base.num_cols, _p(x_star), _p(lo), _p(hi), _p(cols))
+    if cnt < 0:
+        raise ValueError("lpgen_tighten_bounds failed")
+    v = base.copy()
+    v.var_lower, v.var_upper = lo, hi
+    v.name = f"{base.name}-node{seed}"
+    return v, cols[:cnt].copy()
+
+
+def uniform_int(seed: int, index: int, lo: int, hi: int) -> int:
+    return int(_lib.lpgen().lpgen_uniform_int(seed, index, lo, hi))

@@ -1,0 +1,245 @@
+"""Python binding of the CPU checkers -- TEST INFRASTRUCTURE ONLY.
+
+* ``OraclePort``: the C restatement of the reference's PDLP path
+  (oracle/pdlp_oracle.c, built to oracle/build/liboracle_pdlp.so).
+* ``ReferencePdlp``: the reference's own solve_pdlp / equilibrate_model /
+  verify_primal / parse_mps, compiled from its sources into
+  oracle/_ref/libref_pdlp.so by oracle/Makefile (absent where the reference
+  sources were never available; the built library travels with the repo).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU baseline use this
+module, as the checker; the engine never calls it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+import sys
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parent
+sys.path.insert(0, str(ROOT / "markov-zip1_b200"))
+
+from mcpdlp import _abi  # noqa: E402
+from mcpdlp.model import Model  # noqa: E402
+
+ORACLE_LIB = HERE / "build" / "liboracle_pdlp.so"
+REF_LIB = HERE / "_ref" / "libref_pdlp.so"
+REFERENCE_SOURCES = Path("/root/reference")
+
+_VP = C.c_void_p
+
+
+def build(reference: bool | None = None) -> None:
+    """Build the oracle port, and the reference library when its sources exist."""
+    targets = ["oracle"]
+    if reference is None:
+        reference = (REFERENCE_SOURCES / "src" / "lp" / "first_order" / "pdlp.cpp").exists()
+    if reference:
+        targets.append("ref")
+    subprocess.run(["make", "-C", str(HERE), *targets], check=True, capture_output=True)
+
+
+@dataclass
+class CpuSolve:
+    status: int
+    objective: float
+    primal_infeasibility: float
+    dual_infeasibility: float
+    duality_gap: float
+    iterations: int
+    message: str
+    total_ms: float
+    restarts: int
+    ruiz_iterations_executed: int
+    primal: np.ndarray
+    dual: np.ndarray
+    trace: dict | None = None
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+def _result(res: _abi.McPdlpResult, x, y, trace=None) -> CpuSolve:
+    return CpuSolve(res.status, res.objective, res.primal_infeasibility,
+                    res.dual_infeasibility, res.duality_gap, res.iterations,
+                    res.message.decode(), res.total_ms, res.restarts,
+                    res.ruiz_iterations_executed, x, y, trace)
+
+
+def make_trace(capacity: int):
+    arrays = dict(iteration=np.zeros(capacity, np.int64),
+                  primal_infeasibility=np.zeros(capacity),
+                  dual_infeasibility=np.zeros(capacity),
+                  duality_gap=np.zeros(capacity),
+                  step_size=np.zeros(capacity),
+                  primal_weight=np.zeros(capacity),
+                  restarted=np.zeros(capacity, np.int32))
+    t = _abi.McPdlpTrace()
+    t.capacity = capacity
+    t.count = 0
+    for k, a in arrays.items():
+        setattr(t, k, a.ctypes.data)
+    return t, arrays
+
+
+def trace_dict(t, arrays) -> dict:
+    return {k: a[: t.count].copy() for k, a in arrays.items()}
+
+
+class OraclePort:
+    def __init__(self) -> None:
+        if not ORACLE_LIB.exists():
+            build(reference=False)
+        lib = C.CDLL(str(ORACLE_LIB))
+        lib.oracle_solve_pdlp.argtypes = [_VP] * 8
+        lib.oracle_solve_pdlp.restype = C.c_int
+        lib.oracle_equilibrate.argtypes = [C.c_int32, C.c_int32] + [_VP] * 8 + [
+            C.c_int64, C.c_double, _VP, _VP, _VP, _VP]
+        lib.oracle_equilibrate.restype = C.c_int
+        lib.oracle_spmv.argtypes = [C.c_int32, C.c_int32] + [_VP] * 5
+        lib.oracle_spmv.restype = None
+        lib.oracle_spmv_t.argtypes = [C.c_int32, C.c_int32] + [_VP] * 5
+        lib.oracle_spmv_t.restype = None
+        self.lib = lib
+
+    def solve(self, model: Model, options: _abi.McPdlpOptions, warm_x=None, warm_y=None,
+              trace_capacity: int = 0) -> CpuSolve:
+        lp = model.to_struct()
+        x = np.zeros(model.num_cols)
+        y = np.zeros(model.num_rows)
+        res = _abi.McPdlpResult()
+        tr, arrays = make_trace(trace_capacity) if trace_capacity else (None, None)
+        rc = self.lib.oracle_solve_pdlp(C.addressof(lp), C.addressof(options), _ptr(warm_x),
+                                        _ptr(warm_y), _ptr(x), _ptr(y), C.addressof(res),
+                                        C.addressof(tr) if tr is not None else None)
+        if rc != 0:
+            raise RuntimeError(f"oracle_solve_pdlp failed ({rc})")
+        return _result(res, x, y, trace_dict(tr, arrays) if tr is not None else None)
+
+    def equilibrate(self, model: Model, max_iterations: int = 10):
+        v = model.value.copy()
+        obj = model.objective.copy()
+        vl, vu = model.var_lower.copy(), model.var_upper.copy()
+        rl, ru = model.row_lower.copy(), model.row_upper.copy()
+        rs = np.zeros(model.num_rows)
+        cs = np.zeros(model.num_cols)
+        it = C.c_int64(0)
+        conv = C.c_int32(0)
+        rc = self.lib.oracle_equilibrate(model.num_rows, model.num_cols, _ptr(model.col_start),
+                                         _ptr(model.row_index), _ptr(v), _ptr(obj), _ptr(vl),
+                                         _ptr(vu), _ptr(rl), _ptr(ru), max_iterations, 1e-3,
+                                         _ptr(rs), _ptr(cs), C.addressof(it), C.addressof(conv))
+        if rc != 0:
+            raise RuntimeError("oracle_equilibrate failed")
+        return dict(value=v, objective=obj, var_lower=vl, var_upper=vu, row_lower=rl,
+                    row_upper=ru, row_scale=rs, col_scale=cs, iterations=it.value,
+                    converged=bool(conv.value))
+
+    def spmv(self, model: Model, x: np.ndarray) -> np.ndarray:
+        y = np.zeros(model.num_rows)
+        self.lib.oracle_spmv(model.num_rows, model.num_cols, _ptr(model.col_start),
+                             _ptr(model.row_index), _ptr(model.value), _ptr(x), _ptr(y))
+        return y
+
+    def spmv_t(self, model: Model, y: np.ndarray) -> np.ndarray:
+        z = np.zeros(model.num_cols)
+        self.lib.oracle_spmv_t(model.num_rows, model.num_cols, _ptr(model.col_start),
+                               _ptr(model.row_index), _ptr(model.value), _ptr(y), _ptr(z))
+        return z
+
+
+class ReferencePdlp:
+    """The reference's compiled CPU code; ``available()`` is False if not built."""
+
+    @staticmethod
+    def available() -> bool:
+        return REF_LIB.exists()
+
+    def __init__(self) -> None:
+        if not REF_LIB.exists():
+            raise FileNotFoundError(f"{REF_LIB} is not built")
+        lib = C.CDLL(str(REF_LIB))
+        lib.ref_solve_pdlp.argtypes = [_VP] * 5
+        lib.ref_solve_pdlp.restype = C.c_int
+        lib.ref_equilibrate_model.argtypes = [_VP, C.c_int64] + [_VP] * 10
+        lib.ref_equilibrate_model.restype = C.c_int
+        lib.ref_verify_primal.argtypes = [_VP, _VP, C.c_double, C.c_double, _VP, _VP, _VP, _VP]
+        lib.ref_verify_primal.restype = C.c_int
+        lib.ref_mps_load.argtypes = [C.c_char_p, _VP, _VP, _VP, _VP, _VP]
+        lib.ref_mps_load.restype = C.c_int
+        lib.ref_mps_fetch.argtypes = [_VP] * 8
+        lib.ref_mps_fetch.restype = C.c_int
+        lib.ref_last_error.argtypes = [C.c_char_p, C.c_size_t]
+        lib.ref_last_error.restype = C.c_int
+        self.lib = lib
+
+    def _err(self) -> str:
+        b = C.create_string_buffer(512)
+        self.lib.ref_last_error(b, 512)
+        return b.value.decode()
+
+    def solve(self, model: Model, options: _abi.McPdlpOptions) -> CpuSolve:
+        lp = model.to_struct()
+        x = np.zeros(model.num_cols)
+        y = np.zeros(model.num_rows)
+        res = _abi.McPdlpResult()
+        rc = self.lib.ref_solve_pdlp(C.addressof(lp), C.addressof(options), _ptr(x), _ptr(y),
+                                     C.addressof(res))
+        if rc != 0:
+            raise RuntimeError(f"reference solve_pdlp threw: {self._err()}")
+        return _result(res, x, y)
+
+    def equilibrate(self, model: Model, max_iterations: int = 10):
+        lp = model.to_struct()
+        v = np.zeros(model.nnz)
+        obj = np.zeros(model.num_cols)
+        vl, vu = np.zeros(model.num_cols), np.zeros(model.num_cols)
+        rl, ru = np.zeros(model.num_rows), np.zeros(model.num_rows)
+        rs, cs = np.zeros(model.num_rows), np.zeros(model.num_cols)
+        it = C.c_int64(0)
+        conv = C.c_int32(0)
+        rc = self.lib.ref_equilibrate_model(C.addressof(lp), max_iterations, _ptr(v), _ptr(obj),
+                                            _ptr(vl), _ptr(vu), _ptr(rl), _ptr(ru), _ptr(rs),
+                                            _ptr(cs), C.addressof(it), C.addressof(conv))
+        if rc != 0:
+            raise RuntimeError(f"reference equilibrate_model threw: {self._err()}")
+        return dict(value=v, objective=obj, var_lower=vl, var_upper=vu, row_lower=rl,
+                    row_upper=ru, row_scale=rs, col_scale=cs, iterations=it.value,
+                    converged=bool(conv.value))
+
+    def verify_primal(self, model: Model, primal: np.ndarray, claimed: float, tol: float):
+        lp = model.to_struct()
+        passed = C.c_int32(0)
+        rv, vv, ro = C.c_double(0), C.c_double(0), C.c_double(0)
+        rc = self.lib.ref_verify_primal(C.addressof(lp), _ptr(np.ascontiguousarray(primal)),
+                                        claimed, tol, C.addressof(passed), C.addressof(rv),
+                                        C.addressof(vv), C.addressof(ro))
+        if rc != 0:
+            raise RuntimeError(f"reference verify_primal threw: {self._err()}")
+        return dict(passed=bool(passed.value), max_row_violation=rv.value,
+                    max_var_violation=vv.value, recomputed_objective=ro.value)
+
+    def parse_mps(self, path: str | Path) -> Model:
+        m, n, s = C.c_int32(0), C.c_int32(0), C.c_int32(0)
+        nnz = C.c_int64(0)
+        off = C.c_double(0)
+        rc = self.lib.ref_mps_load(str(path).encode(), C.addressof(m), C.addressof(n),
+                                   C.addressof(nnz), C.addressof(s), C.addressof(off))
+        if rc != 0:
+            raise RuntimeError(f"reference parse_mps threw: {self._err()}")
+        M, N, Z = m.value, n.value, nnz.value
+        cs = np.zeros(N + 1, np.int32)
+        ri = np.zeros(Z, np.int32)
+        v = np.zeros(Z)
+        obj, vl, vu = np.zeros(N), np.zeros(N), np.zeros(N)
+        rl, ru = np.zeros(M), np.zeros(M)
+        self.lib.ref_mps_fetch(_ptr(cs), _ptr(ri), _ptr(v), _ptr(obj), _ptr(vl), _ptr(vu),
+                               _ptr(rl), _ptr(ru))
+        return Model(M, N, cs, ri, v, obj, vl, vu, rl, ru, off.value, s.value,
+                     name=Path(path).stem)

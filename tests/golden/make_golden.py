@@ -1,0 +1,137 @@
+"""Generate the golden fixtures of the PDLP path from the reference itself.
+
+Run in a checkout where the reference sources exist (oracle/Makefile builds
+oracle/_ref/libref_pdlp.so from them):
+
+    python tests/golden/make_golden.py
+
+Writes, next to this script:
+  * <name>.npz   -- small LPs in CSC form (the reference's PDLP unit-test
+                   models, tests/pdlp_test.cpp:12-129; the ADR-P3-05 model
+                   examples/phase3/tiny_simplex.mps; Netlib models from
+                   data/netlib that the reference PDLP solves), parsed by the
+                   reference's own MPS reader;
+  * golden.json  -- the reference solve_pdlp result on each (status,
+                   iterations, objective, residuals, SHA-256 of the primal and
+                   dual bytes) at 1e-4 and 1e-8, the same for seeded synthetic
+                   LPs (regenerated from their seed, pinned by a SHA-256 of the
+                   generated arrays), and equilibrate_model digests.
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parent.parent
+sys.path.insert(0, str(ROOT / "markov-zip1_b200"))
+sys.path.insert(0, str(ROOT / "oracle"))
+
+from mcpdlp import _abi, generators  # noqa: E402
+from mcpdlp.model import Model, from_triplets  # noqa: E402
+import oracle as orc  # noqa: E402
+
+REF = Path("/root/reference")
+NETLIB = ["afiro", "sc50a", "sc50b", "sc105", "blend", "recipe", "scsd1", "scsd6"]
+SYNTHETIC = [  # (name, seed, m, n, k, family)
+    ("config0_s1", 1, 1000, 3000, 6, "standard"),
+    ("config0_s2", 2, 1000, 3000, 6, "standard"),
+    ("config0_s3", 3, 1000, 3000, 6, "standard"),
+    ("small_s7", 7, 200, 600, 6, "standard"),
+    ("precision_s1", 1, 300, 900, 10, "precision"),
+]
+TOLS = [1e-4, 1e-8]
+
+
+def sha(*arrays) -> str:
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+def model_digest(m: Model) -> str:
+    return sha(m.col_start, m.row_index, m.value, m.objective, m.var_lower, m.var_upper,
+               m.row_lower, m.row_upper)
+
+
+def blend_lp() -> Model:
+    # tests/pdlp_test.cpp:12-48: min -x1 - 2 x2, x1 + x2 <= 4, x1 <= 3, x2 <= 3, 0 <= x <= 10
+    inf = np.inf
+    return from_triplets(3, 2, [0, 0, 1, 2], [0, 1, 0, 1], [1.0, 1.0, 1.0, 1.0],
+                         objective=[-1.0, -2.0], var_lower=[0.0, 0.0], var_upper=[10.0, 10.0],
+                         row_lower=[-inf, -inf, -inf], row_upper=[4.0, 3.0, 3.0], name="blend_pdlp")
+
+
+def equality_lp() -> Model:
+    # tests/pdlp_test.cpp:82-109: min x1 + x2, x1 + x2 = 5, 0 <= x <= 5
+    return from_triplets(1, 2, [0, 0], [0, 1], [1.0, 1.0], objective=[1.0, 1.0],
+                         var_lower=[0.0, 0.0], var_upper=[5.0, 5.0], row_lower=[5.0],
+                         row_upper=[5.0], name="equality_pdlp")
+
+
+def save_model(m: Model, name: str) -> None:
+    np.savez_compressed(HERE / f"{name}.npz", num_rows=m.num_rows, num_cols=m.num_cols,
+                        col_start=m.col_start, row_index=m.row_index, value=m.value,
+                        objective=m.objective, var_lower=m.var_lower, var_upper=m.var_upper,
+                        row_lower=m.row_lower, row_upper=m.row_upper,
+                        objective_offset=m.objective_offset, objective_sense=int(m.objective_sense))
+
+
+def opts(tol: float, max_iter: int = 100000):
+    o = _abi.default_options_struct()
+    o.primal_tolerance = o.dual_tolerance = o.gap_tolerance = tol
+    o.max_iterations = max_iter
+    return o
+
+
+def record(ref, m: Model) -> dict:
+    out = {}
+    for tol in TOLS:
+        r = ref.solve(m, opts(tol))
+        out[f"{tol:g}"] = dict(status=r.status, iterations=r.iterations, objective=r.objective,
+                               primal_infeasibility=r.primal_infeasibility,
+                               dual_infeasibility=r.dual_infeasibility, duality_gap=r.duality_gap,
+                               primal_sha256=sha(r.primal), dual_sha256=sha(r.dual),
+                               message=r.message)
+    return out
+
+
+def main() -> None:
+    orc.build(reference=True)
+    ref = orc.ReferencePdlp()
+    golden = {"models": {}, "synthetic": {}, "ruiz": {}}
+    fixtures = [blend_lp(), equality_lp(), ref.parse_mps(REF / "examples/phase3/tiny_simplex.mps")]
+    fixtures[2].name = "tiny_simplex"
+    for name in NETLIB:
+        mm = ref.parse_mps(REF / "data/netlib" / f"{name}.mps")
+        mm.name = f"netlib_{name}"
+        fixtures.append(mm)
+    for m in fixtures:
+        save_model(m, m.name)
+        golden["models"][m.name] = dict(file=f"{m.name}.npz", m=m.num_rows, n=m.num_cols,
+                                        nnz=m.nnz, digest=model_digest(m), results=record(ref, m))
+        print(m.name, {k: (v["status"], v["iterations"], v["objective"])
+                       for k, v in golden["models"][m.name]["results"].items()})
+    for name, seed, mm, nn, kk, fam in SYNTHETIC:
+        m = generators.random_lp(seed, mm, nn, kk, fam)
+        golden["synthetic"][name] = dict(seed=seed, m=mm, n=nn, k=kk, family=fam,
+                                         digest=model_digest(m), optimum=m.info["optimum"],
+                                         results=record(ref, m))
+        print(name, {k: (v["status"], v["iterations"], v["objective"])
+                     for k, v in golden["synthetic"][name]["results"].items()})
+        e = ref.equilibrate(m, 10)
+        golden["ruiz"][name] = dict(iterations=e["iterations"], converged=e["converged"],
+                                    value_sha256=sha(e["value"]),
+                                    scales_sha256=sha(e["row_scale"], e["col_scale"]),
+                                    bounds_sha256=sha(e["objective"], e["var_lower"], e["var_upper"],
+                                                      e["row_lower"], e["row_upper"]))
+    (HERE / "golden.json").write_text(json.dumps(golden, indent=1, sort_keys=True))
+
+
+if __name__ == "__main__":
+    main()
