@@ -142,14 +142,20 @@ def test_empty_rows_and_columns(gpu_ctx, oracle):
 
 
 def test_maximize_with_offset(gpu_ctx, oracle):
+    """Maximise + offset.  The reference's duality gap adds the raw (maximise)
+    objective to a minimisation-sign dual objective (pdlp.cpp:113-131), so a
+    maximise LP with a nonzero optimum never meets the gap test and ends at
+    the iteration limit; the engine reproduces that status and the iterate."""
     m = synthetic("small_s7")
     m.objective = -m.objective
     m.objective_sense = mcpdlp.ObjectiveSense.maximize
     m.objective_offset = 12.5
-    cpu = oracle.solve(m, options(1e-8))
-    res = gpu_ctx.solve(m, gpu_opts(1e-8))
-    assert res.status == cpu.status == PdlpStatus.optimal
+    cpu = oracle.solve(m, options(1e-8, max_iterations=4000))
+    res = gpu_ctx.solve(m, gpu_opts(1e-8, max_iterations=4000))
+    assert res.status == cpu.status == PdlpStatus.iteration_limit
+    assert res.iterations == cpu.iterations == 4000
     assert rel(res.objective, cpu.objective) <= 1e-6
+    assert rel(res.duality_gap, cpu.duality_gap) <= 1e-6
 
 
 def test_deterministic(gpu_ctx):
