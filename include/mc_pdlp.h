@@ -108,7 +108,11 @@ typedef struct mc_pdlp_options {
     int32_t refine_max_rounds;        /* FP32_REFINE: outer refinement rounds, default 12 */
     double refine_inner_tolerance;    /* FP32_REFINE: inner relative KKT target, default 1e-4 */
     int32_t check_every_chunks;       /* host status poll interval in restart chunks, default 1 */
-    int32_t reserved_i[7];
+    int32_t lanes_per_column;         /* A^T y kernel: 0 = chosen by mean column length,
+                                         -1 = one thread per column over shared-memory
+                                         tiles, 1..32 (power of two) = lanes per column */
+    int32_t lanes_per_row;            /* A x kernel, same meaning per row */
+    int32_t reserved_i[5];
     double reserved_d[8];
 } mc_pdlp_options;
 

@@ -51,6 +51,39 @@ struct DevState {
     int pad[3];
 };
 
+// ---- cache policy helpers -------------------------------------------------
+// The matrix and the per-line vectors are streamed once per iteration: they
+// are loaded with the "streaming" (evict-first) hint so that they do not push
+// the gathered iterate (x-bar, 40 MB at 5M columns; y, 16 MB at 2M rows) out
+// of L2.  The gathered iterate is written and read with an L2 evict_last
+// policy so that it stays resident between the kernel that writes it and the
+// kernel that gathers from it.
+__device__ __forceinline__ unsigned long long policy_keep() {
+    unsigned long long p;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ double ld_keep(const double* a, unsigned long long pol) {
+    double v;
+    asm("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ float ld_keep(const float* a, unsigned long long pol) {
+    float v;
+    asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ void st_keep(double* a, double v, unsigned long long pol) {
+    asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(a), "d"(v), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void st_keep(float* a, float v, unsigned long long pol) {
+    asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(a), "f"(v), "l"(pol) : "memory");
+}
+template <class T>
+__device__ __forceinline__ T ld_stream(const T* a) { return __ldcs(a); }
+template <class T>
+__device__ __forceinline__ void st_stream(T* a, T v) { __stcs(a, v); }
+
 // std::clamp(v, lo, hi): lo if v < lo, hi if hi < v, else v.
 template <class T>
 __device__ __forceinline__ T clampv(T v, T lo, T hi) {

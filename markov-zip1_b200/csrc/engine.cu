@@ -171,10 +171,11 @@ int blocks_for(const Ctx& ctx, long long work_items, int per_block) {
     return (int)b;
 }
 
+// Lanes per line for the lane kernels: each lane should carry about four
+// entries (four loads in flight per step), up to a warp per line.
 int pick_lanes(double mean_len) {
-    const double half = mean_len / 2.0;
     int g = 1;
-    while (g < 32 && 2.0 * g <= half) g *= 2;
+    while (g < 32 && 4.0 * (2 * g) <= mean_len) g *= 2;
     return g;
 }
 

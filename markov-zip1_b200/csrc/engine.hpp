@@ -6,6 +6,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <map>
 #include <vector>
@@ -97,6 +98,30 @@ struct Ctx {
 };
 
 int blocks_for(const Ctx& ctx, long long work_items, int per_block);
+
+// Grid for a grid-stride kernel: one full wave of resident blocks (from the
+// kernel's own occupancy), never more than the work needs.
+template <class K>
+int grid_for(const Ctx& ctx, K kernel, long long work_items, int per_block, size_t smem = 0) {
+    static thread_local std::map<const void*, int> cache;
+    const void* key = reinterpret_cast<const void*>(kernel);
+    auto it = cache.find(key);
+    int per_sm = 0;
+    if (it == cache.end()) {
+        if (smem > 0) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, smem) != cudaSuccess ||
+            per_sm < 1)
+            per_sm = 1;
+        cache[key] = per_sm;
+    } else {
+        per_sm = it->second;
+    }
+    long long b = (work_items + per_block - 1) / per_block;
+    const long long cap = std::min<long long>((long long)ctx.sm_count * per_sm, kMaxPartials / 2);
+    if (b > cap) b = cap;
+    if (b < 1) b = 1;
+    return (int)b;
+}
 int pick_lanes(double mean_len);
 
 int solve_fp32_refine(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* warm_x,

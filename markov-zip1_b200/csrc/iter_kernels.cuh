@@ -78,24 +78,29 @@ template <> __device__ __forceinline__ double div_rn(double a, double b) { retur
 template <> __device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
 
 // Dot of line `j` of a compressed matrix with vector v, G lanes per line,
-// two independent accumulators per lane for memory-level parallelism.
+// four independent loads/gathers in flight per lane per step.  The matrix is
+// streamed (evict-first); v is gathered with the keep policy.
 template <int G, class T>
 __device__ __forceinline__ T line_dot(const int* __restrict__ start, const int* __restrict__ idx,
                                       const T* __restrict__ val, const T* __restrict__ v, int j,
-                                      bool valid, int sub) {
-    T s0 = T(0), s1 = T(0);
+                                      bool valid, int sub, unsigned long long pol) {
+    T s0 = T(0), s1 = T(0), s2 = T(0), s3 = T(0);
     if (valid) {
-        const int b = start[j], e = start[j + 1];
+        const int b = __ldg(start + j), e = __ldg(start + j + 1);
         int p = b + sub;
-        for (; p + G < e; p += 2 * G) {
-            const int i0 = __ldg(idx + p), i1 = __ldg(idx + p + G);
-            const T a0 = __ldg(val + p), a1 = __ldg(val + p + G);
-            s0 = fma(a0, v[i0], s0);
-            s1 = fma(a1, v[i1], s1);
+        for (; p + 3 * G < e; p += 4 * G) {
+            const int i0 = ld_stream(idx + p), i1 = ld_stream(idx + p + G);
+            const int i2 = ld_stream(idx + p + 2 * G), i3 = ld_stream(idx + p + 3 * G);
+            const T a0 = ld_stream(val + p), a1 = ld_stream(val + p + G);
+            const T a2 = ld_stream(val + p + 2 * G), a3 = ld_stream(val + p + 3 * G);
+            s0 = fma(a0, ld_keep(v + i0, pol), s0);
+            s1 = fma(a1, ld_keep(v + i1, pol), s1);
+            s2 = fma(a2, ld_keep(v + i2, pol), s2);
+            s3 = fma(a3, ld_keep(v + i3, pol), s3);
         }
-        if (p < e) s0 = fma(__ldg(val + p), v[__ldg(idx + p)], s0);
+        for (; p < e; p += G) s0 = fma(ld_stream(val + p), ld_keep(v + ld_stream(idx + p), pol), s0);
     }
-    return group_sum<G>(s0 + s1);
+    return group_sum<G>((s0 + s1) + (s2 + s3));
 }
 
 // Two dots of the same line (A x-bar and A dx on step-size iterations).
@@ -103,15 +108,15 @@ template <int G, class T>
 __device__ __forceinline__ void line_dot2(const int* __restrict__ start, const int* __restrict__ idx,
                                           const T* __restrict__ val, const T* __restrict__ v,
                                           const T* __restrict__ w, int j, bool valid, int sub,
-                                          T& out_v, T& out_w) {
+                                          T& out_v, T& out_w, unsigned long long pol) {
     T sv = T(0), sw = T(0);
     if (valid) {
-        const int b = start[j], e = start[j + 1];
+        const int b = __ldg(start + j), e = __ldg(start + j + 1);
         for (int p = b + sub; p < e; p += G) {
-            const int i = __ldg(idx + p);
-            const T a = __ldg(val + p);
-            sv = fma(a, v[i], sv);
-            sw = fma(a, w[i], sw);
+            const int i = ld_stream(idx + p);
+            const T a = ld_stream(val + p);
+            sv = fma(a, ld_keep(v + i, pol), sv);
+            sw = fma(a, __ldg(w + i), sw);
         }
     }
     out_v = group_sum<G>(sv);
@@ -127,10 +132,11 @@ __global__ void __launch_bounds__(kBlock) k_spmv(int rows, const int* __restrict
     const int lane = threadIdx.x & 31, sub = lane % G, slot = lane / G;
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const unsigned long long pol = policy_keep();
     for (long long t = warp; t * LPW < rows; t += nwarps) {
         const int i = (int)(t * LPW) + slot;
         const bool valid = i < rows;
-        const T s = line_dot<G>(start, idx, val, x, i, valid, sub);
+        const T s = line_dot<G>(start, idx, val, x, i, valid, sub, pol);
         if (valid && sub == 0) y[i] = s;
     }
 }
@@ -149,26 +155,36 @@ __global__ void __launch_bounds__(kBlock) k_primal(Iterates<T> P, int k) {
     const int lane = threadIdx.x & 31, sub = lane % G, slot = lane / G;
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const unsigned long long pol = policy_keep();
     double acc = 0.0;
     for (long long t = warp; t * LPW < P.n; t += nwarps) {
         const int j = (int)(t * LPW) + slot;
         const bool valid = j < P.n;
-        const T aty = line_dot<G>(P.csc_start, P.csc_row, P.csc_val, P.y, j, valid, sub);
-        if (valid && sub == 0) {
-            const T g = add_rn(P.c[j], aty);
-            const T tau = div_rn(step, P.col_norm[j]);
-            const T xo = P.x[j];
-            const T xp = clampv(sub_rn(xo, mul_rn(tau, g)), P.lo[j], P.hi[j]);
+        const bool owner = valid && sub == 0;
+        // the line's own vector entries are loaded before the SpMV so that
+        // their latency overlaps the matrix stream and the gathers
+        T cn = T(1), cj = T(0), xo = T(0), lj = T(0), hj = T(0), xa = T(0);
+        if (owner) {
+            cn = ld_stream(P.col_norm + j);
+            cj = ld_stream(P.c + j);
+            xo = ld_stream(P.x + j);
+            lj = ld_stream(P.lo + j);
+            hj = ld_stream(P.hi + j);
+            xa = ld_stream(P.x_avg + j);
+        }
+        const T aty = line_dot<G>(P.csc_start, P.csc_row, P.csc_val, P.y, j, valid, sub, pol);
+        if (owner) {
+            const T g = add_rn(cj, aty);
+            const T tau = div_rn(step, cn);
+            const T xp = clampv(sub_rn(xo, mul_rn(tau, g)), lj, hj);
             const T d = sub_rn(xp, xo);
             if (STEP) {
-                P.dx[j] = d;
-                const double cn = (double)P.col_norm[j];
-                acc += __dmul_rn(__dmul_rn(cn, (double)d), (double)d);
+                st_keep(P.dx + j, d, pol);
+                acc += __dmul_rn(__dmul_rn((double)cn, (double)d), (double)d);
             }
-            P.x[j] = xp;
-            P.x_bar[j] = sub_rn(mul_rn(T(2), xp), xo);
-            const T xa = P.x_avg[j];
-            P.x_avg[j] = add_rn(xa, div_rn(sub_rn(xp, xa), cnt));
+            st_stream(P.x + j, xp);
+            st_keep(P.x_bar + j, sub_rn(mul_rn(T(2), xp), xo), pol);
+            st_stream(P.x_avg + j, add_rn(xa, div_rn(sub_rn(xp, xa), cnt)));
         }
     }
     if (STEP) {
@@ -180,15 +196,29 @@ __global__ void __launch_bounds__(kBlock) k_primal(Iterates<T> P, int k) {
 // ------------------------------------------------------------------- dual
 // v = y + sigma (A x-bar); y+ = v - sigma clamp(v/sigma, b_lo, b_hi); y_avg
 // (pdlp.cpp:220-224, :227)
+// The row's own vector entries, loaded ahead of the SpMV.
 template <class T>
-__device__ __forceinline__ void dual_update(const Iterates<T>& P, int i, T ax, T sg, T cnt) {
-    const T sigma = div_rn(sg, P.row_norm[i]);
-    const T yo = P.y[i];
-    const T v = add_rn(yo, mul_rn(sigma, ax));
-    const T yn = sub_rn(v, mul_rn(sigma, clampv(div_rn(v, sigma), P.blo[i], P.bhi[i])));
-    P.y[i] = yn;
-    const T ya = P.y_avg[i];
-    P.y_avg[i] = add_rn(ya, div_rn(sub_rn(yn, ya), cnt));
+struct RowData {
+    T rn, yo, bl, bh, ya;
+};
+template <class T>
+__device__ __forceinline__ RowData<T> load_row(const Iterates<T>& P, int i) {
+    return RowData<T>{ld_stream(P.row_norm + i), ld_stream(P.y + i), ld_stream(P.blo + i), ld_stream(P.bhi + i),
+                      ld_stream(P.y_avg + i)};
+}
+template <class T>
+__device__ __forceinline__ void dual_update(const Iterates<T>& P, int i, const RowData<T>& r, T ax, T sg, T cnt,
+                                            unsigned long long pol) {
+    const T sigma = div_rn(sg, r.rn);
+    const T v = add_rn(r.yo, mul_rn(sigma, ax));
+    const T yn = sub_rn(v, mul_rn(sigma, clampv(div_rn(v, sigma), r.bl, r.bh)));
+    st_keep(P.y + i, yn, pol);
+    st_stream(P.y_avg + i, add_rn(r.ya, div_rn(sub_rn(yn, r.ya), cnt)));
+}
+template <class T>
+__device__ __forceinline__ void dual_update(const Iterates<T>& P, int i, T ax, T sg, T cnt,
+                                            unsigned long long pol) {
+    dual_update(P, i, load_row(P, i), ax, sg, cnt, pol);
 }
 
 template <int G, class T>
@@ -201,11 +231,14 @@ __global__ void __launch_bounds__(kBlock) k_dual(Iterates<T> P, int k) {
     const int lane = threadIdx.x & 31, sub = lane % G, slot = lane / G;
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const unsigned long long pol = policy_keep();
     for (long long t = warp; t * LPW < P.m; t += nwarps) {
         const int i = (int)(t * LPW) + slot;
         const bool valid = i < P.m;
-        const T ax = line_dot<G>(P.csr_start, P.csr_col, P.csr_val, P.x_bar, i, valid, sub);
-        if (valid && sub == 0) dual_update(P, i, ax, sg, cnt);
+        RowData<T> r{};
+        if (valid && sub == 0) r = load_row(P, i);
+        const T ax = line_dot<G>(P.csr_start, P.csr_col, P.csr_val, P.x_bar, i, valid, sub, pol);
+        if (valid && sub == 0) dual_update(P, i, r, ax, sg, cnt, pol);
     }
 }
 
@@ -220,12 +253,13 @@ __global__ void __launch_bounds__(kBlock) k_dual_probe(Iterates<T> P) {
     const int lane = threadIdx.x & 31, sub = lane % G, slot = lane / G;
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const unsigned long long pol = policy_keep();
     double acc = 0.0;
     for (long long t = warp; t * LPW < P.m; t += nwarps) {
         const int i = (int)(t * LPW) + slot;
         const bool valid = i < P.m;
         T axb, adx;
-        line_dot2<G>(P.csr_start, P.csr_col, P.csr_val, P.x_bar, P.dx, i, valid, sub, axb, adx);
+        line_dot2<G>(P.csr_start, P.csr_col, P.csr_val, P.x_bar, P.dx, i, valid, sub, axb, adx, pol);
         if (valid && sub == 0) {
             P.ax_bar[i] = axb;
             const double a = (double)adx;
@@ -261,8 +295,9 @@ __global__ void __launch_bounds__(kBlock) k_dual_apply(Iterates<T> P, int k) {
     if (st->done) return;
     const T sg = T(st->eta * st->omega);
     const T cnt = T((double)(st->avg_count + k + 1));
+    const unsigned long long pol = policy_keep();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.m; i += gridDim.x * blockDim.x)
-        dual_update(P, i, P.ax_bar[i], sg, cnt);
+        dual_update(P, i, P.ax_bar[i], sg, cnt, pol);
 }
 
 // --------------------------------------------------------------- residuals

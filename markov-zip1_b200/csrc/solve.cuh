@@ -4,6 +4,7 @@
 #include "engine.hpp"
 #include "iter_kernels.cuh"
 #include "setup_kernels.cuh"
+#include "staged.cuh"
 
 #include <cmath>
 #include <cstring>
@@ -20,22 +21,79 @@ namespace mc {
         default: { constexpr int G = 32; __VA_ARGS__; } break; \
     }
 
-// Launch geometry of one problem: lanes per column/row and grid sizes.
+// Launch geometry of one problem: per side either the tile-staged kernels
+// (one thread per line, matrix through shared memory) or the lane kernels
+// (G lanes per line, for long lines), and grid sizes (one wave of resident
+// blocks per kernel; the reduction partial counts follow the grids, so they
+// are fixed per plan).
 struct Plan {
+    bool staged_col = false, staged_row = false;
     int g_col = 1, g_row = 1;
-    int nb_col = 1, nb_row = 1;  // SpMV kernels over columns / rows
-    int nb_m = 1, nb_nm = 1;     // elementwise kernels over m / n+m
+    int nb_col = 1, nb_row = 1;           // primal / dual SpMV kernels
+    int nb_col_step = 1, nb_row_step = 1; // step-size variants (they write partials)
+    int nb_res_col = 1, nb_res_row = 1;   // residual kernels
+    int nb_m = 1, nb_nm = 1;              // elementwise kernels over m / n+m
+    Tiles tiles{};
 };
 
-Plan make_plan(const Ctx& ctx, int m, int n, long long nnz) {
+static int valid_lanes(int g) { return g == 1 || g == 2 || g == 4 || g == 8 || g == 16 || g == 32; }
+
+// lanes option: 0 = lanes chosen by mean line length, -1 = staged, 1..32 = lanes
+
+template <class T>
+Plan make_plan(const Ctx& ctx, int m, int n, long long nnz, int force_col, int force_row,
+               const int* col_bounds, const int* row_bounds) {
     Plan p;
-    p.g_col = pick_lanes(n > 0 ? (double)nnz / n : 1.0);
-    p.g_row = pick_lanes(m > 0 ? (double)nnz / m : 1.0);
-    p.nb_col = blocks_for(ctx, n, kBlock / p.g_col);
-    p.nb_row = blocks_for(ctx, m, kBlock / p.g_row);
-    p.nb_m = blocks_for(ctx, m, kBlock);
-    p.nb_nm = blocks_for(ctx, (long long)n + m, kBlock);
+    const double mean_col = n > 0 ? (double)nnz / n : 1.0;
+    const double mean_row = m > 0 ? (double)nnz / m : 1.0;
+    p.staged_col = force_col == -1;
+    p.staged_row = force_row == -1;
+    p.g_col = valid_lanes(force_col) ? force_col : pick_lanes(mean_col);
+    p.g_row = valid_lanes(force_row) ? force_row : pick_lanes(mean_row);
+    const int chunk = stage_chunk<T>();
+    p.tiles.col_bounds = col_bounds;
+    p.tiles.row_bounds = row_bounds;
+    p.tiles.ncol_tiles = (int)std::max<long long>(1, (nnz + chunk - 1) / chunk);
+    p.tiles.nrow_tiles = p.tiles.ncol_tiles;
+    const size_t sm = staged_smem_bytes<T>();
+    if (p.staged_col) {
+        p.nb_col = grid_for(ctx, k_primal_staged<false, T>, p.tiles.ncol_tiles, 1, sm);
+        p.nb_col_step = grid_for(ctx, k_primal_staged<true, T>, p.tiles.ncol_tiles, 1, sm);
+    } else {
+        MC_DISPATCH_G(p.g_col, {
+            p.nb_col = grid_for(ctx, k_primal<G, false, T>, n, kBlock / G);
+            p.nb_col_step = grid_for(ctx, k_primal<G, true, T>, n, kBlock / G);
+        });
+    }
+    if (p.staged_row) {
+        p.nb_row = grid_for(ctx, k_dual_staged<T>, p.tiles.nrow_tiles, 1, sm);
+        p.nb_row_step = grid_for(ctx, k_dual_probe_staged<T>, p.tiles.nrow_tiles, 1, sm);
+    } else {
+        MC_DISPATCH_G(p.g_row, {
+            p.nb_row = grid_for(ctx, k_dual<G, T>, m, kBlock / G);
+            p.nb_row_step = grid_for(ctx, k_dual_probe<G, T>, m, kBlock / G);
+        });
+    }
+    MC_DISPATCH_G(p.g_col, p.nb_res_col = grid_for(ctx, k_residual_cols<G, T>, n, kBlock / G));
+    MC_DISPATCH_G(p.g_row, p.nb_res_row = grid_for(ctx, k_residual_rows<G, T>, m, kBlock / G));
+    p.nb_m = grid_for(ctx, k_dual_apply<T>, m, kBlock);
+    p.nb_nm = grid_for(ctx, k_restart_copy<T>, (long long)n + m, kBlock);
     return p;
+}
+
+// tile boundaries of both copies (once per solve)
+int build_tiles(Ctx& ctx, const Plan& p, int m, int n, const int* csc_start, const int* csr_start,
+                int* col_bounds, int* row_bounds, int chunk) {
+    cudaStream_t s = ctx.stream;
+    ctx.begin_launch(MC_KERNEL_SETUP);
+    k_tile_bounds<<<(p.tiles.ncol_tiles + kBlock) / kBlock, kBlock, 0, s>>>(n, csc_start, chunk, p.tiles.ncol_tiles,
+                                                                            col_bounds);
+    ctx.end_launch();
+    ctx.begin_launch(MC_KERNEL_SETUP);
+    k_tile_bounds<<<(p.tiles.nrow_tiles + kBlock) / kBlock, kBlock, 0, s>>>(m, csr_start, chunk, p.tiles.nrow_tiles,
+                                                                            row_bounds);
+    ctx.end_launch();
+    return ctx.launch_check("tile bounds");
 }
 
 // ------------------------------------------------------------- transpose
@@ -156,26 +214,32 @@ int ruiz(Ctx& ctx, int m, int n, long long nnz, const int* csc_start, const int*
 template <class T>
 int enqueue_iteration(Ctx& ctx, const Iterates<T>& P, const Plan& pl, int k, bool step, const Controls& ctl) {
     cudaStream_t s = ctx.stream;
+    const size_t sm = staged_smem_bytes<T>();
     ctx.begin_launch(MC_KERNEL_PRIMAL);
-    if (step) {
-        MC_DISPATCH_G(pl.g_col, (k_primal<G, true, T><<<pl.nb_col, kBlock, 0, s>>>(P, k)));
+    if (pl.staged_col) {
+        if (step) k_primal_staged<true, T><<<pl.nb_col_step, kBlock, sm, s>>>(P, pl.tiles, k);
+        else k_primal_staged<false, T><<<pl.nb_col, kBlock, sm, s>>>(P, pl.tiles, k);
+    } else if (step) {
+        MC_DISPATCH_G(pl.g_col, (k_primal<G, true, T><<<pl.nb_col_step, kBlock, 0, s>>>(P, k)));
     } else {
         MC_DISPATCH_G(pl.g_col, (k_primal<G, false, T><<<pl.nb_col, kBlock, 0, s>>>(P, k)));
     }
     ctx.end_launch();
     if (step) {
         ctx.begin_launch(MC_KERNEL_DUAL_STEP);
-        MC_DISPATCH_G(pl.g_row, (k_dual_probe<G, T><<<pl.nb_row, kBlock, 0, s>>>(P)));
+        if (pl.staged_row) k_dual_probe_staged<T><<<pl.nb_row_step, kBlock, sm, s>>>(P, pl.tiles);
+        else MC_DISPATCH_G(pl.g_row, (k_dual_probe<G, T><<<pl.nb_row_step, kBlock, 0, s>>>(P)));
         ctx.end_launch();
         ctx.begin_launch(MC_KERNEL_OTHER);
-        k_step_size<<<1, 1024, 0, s>>>(P.partials, pl.nb_col, pl.nb_row, P.st, ctl);
+        k_step_size<<<1, 1024, 0, s>>>(P.partials, pl.nb_col_step, pl.nb_row_step, P.st, ctl);
         ctx.end_launch();
         ctx.begin_launch(MC_KERNEL_DUAL_STEP);
         k_dual_apply<T><<<pl.nb_m, kBlock, 0, s>>>(P, k);
         ctx.end_launch();
     } else {
         ctx.begin_launch(MC_KERNEL_DUAL);
-        MC_DISPATCH_G(pl.g_row, (k_dual<G, T><<<pl.nb_row, kBlock, 0, s>>>(P, k)));
+        if (pl.staged_row) k_dual_staged<T><<<pl.nb_row, kBlock, sm, s>>>(P, pl.tiles, k);
+        else MC_DISPATCH_G(pl.g_row, (k_dual<G, T><<<pl.nb_row, kBlock, 0, s>>>(P, k)));
         ctx.end_launch();
     }
     return ctx.launch_check("iteration");
@@ -186,13 +250,13 @@ int enqueue_check(Ctx& ctx, const Iterates<T>& P, const Original& O, const Plan&
                   int final_pass, const Controls& ctl, const TraceBuf& tr) {
     cudaStream_t s = ctx.stream;
     ctx.begin_launch(MC_KERNEL_RESIDUAL);
-    MC_DISPATCH_G(pl.g_row, (k_residual_rows<G, T><<<pl.nb_row, kBlock, 0, s>>>(P, O)));
+    MC_DISPATCH_G(pl.g_row, (k_residual_rows<G, T><<<pl.nb_res_row, kBlock, 0, s>>>(P, O)));
     ctx.end_launch();
     ctx.begin_launch(MC_KERNEL_RESIDUAL);
-    MC_DISPATCH_G(pl.g_col, (k_residual_cols<G, T><<<pl.nb_col, kBlock, 0, s>>>(P, O)));
+    MC_DISPATCH_G(pl.g_col, (k_residual_cols<G, T><<<pl.nb_res_col, kBlock, 0, s>>>(P, O)));
     ctx.end_launch();
     ctx.begin_launch(MC_KERNEL_RESIDUAL);
-    k_finalize<<<1, 1024, 0, s>>>(P.partials, pl.nb_row, pl.nb_col, span, final_pass, O.offset, ctl, tr, P.st);
+    k_finalize<<<1, 1024, 0, s>>>(P.partials, pl.nb_res_row, pl.nb_res_col, span, final_pass, O.offset, ctl, tr, P.st);
     ctx.end_launch();
     if (!final_pass) {
         ctx.begin_launch(MC_KERNEL_OTHER);
@@ -266,6 +330,9 @@ int validate_options(const mc_pdlp_options* o) {
         return set_error(MC_ERR_INVALID_ARGUMENT, "unknown restart_strategy %d", o->restart_strategy);
     if (o->precision != MC_PRECISION_FP64 && o->precision != MC_PRECISION_FP32_REFINE)
         return set_error(MC_ERR_INVALID_ARGUMENT, "unknown precision %d", o->precision);
+    if ((o->lanes_per_column && o->lanes_per_column != -1 && !valid_lanes(o->lanes_per_column)) ||
+        (o->lanes_per_row && o->lanes_per_row != -1 && !valid_lanes(o->lanes_per_row)))
+        return set_error(MC_ERR_INVALID_ARGUMENT, "lanes per line must be 0, -1 or a power of two <= 32");
     return MC_OK;
 }
 
@@ -323,12 +390,18 @@ int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* 
     // ---- arena layout
     const long long trace_cap = trace ? trace->capacity : 0;
     Layout L;
-    const size_t o_csc_start = dev_in ? 0 : L.add<int>(n + 1);
-    const size_t o_csc_row = dev_in ? 0 : L.add<int>(nnz);
-    const size_t o_csc_val = L.add<double>(nnz);
+    // structure and values are always copied (the matrix arrays padded by 16
+    // entries so that 16-byte tile copies may overrun nnz)
+    const size_t o_csc_start = L.add<int>(n + 1);
+    const size_t o_csc_row = L.add<int>(nnz + 16);
+    const size_t o_csc_val = L.add<double>(nnz + 16);
     const size_t o_csr_start = L.add<int>(m + 1);
-    const size_t o_csr_col = L.add<int>(nnz);
-    const size_t o_csr_val = L.add<double>(nnz);
+    const size_t o_csr_col = L.add<int>(nnz + 16);
+    const size_t o_csr_val = L.add<double>(nnz + 16);
+    const int chunk = stage_chunk<double>();
+    const long long ntiles = std::max<long long>(1, (nnz + chunk - 1) / chunk);
+    const size_t o_col_bounds = L.add<int>(ntiles + 1);
+    const size_t o_row_bounds = L.add<int>(ntiles + 1);
     const size_t o_cursor = L.add<int>(m);
     const size_t o_long = L.add<int>(m);
     const size_t o_counters = L.add<int>(4);
@@ -353,8 +426,8 @@ int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* 
     char* A = static_cast<char*>(ctx.arena.base);
     auto at = [&](size_t off) { return static_cast<void*>(A + off); };
 
-    const int* csc_start = dev_in ? lp->col_start : static_cast<int*>(at(o_csc_start));
-    const int* csc_row = dev_in ? lp->row_index : static_cast<int*>(at(o_csc_row));
+    const int* csc_start = static_cast<int*>(at(o_csc_start));
+    const int* csc_row = static_cast<int*>(at(o_csc_row));
     double* csc_val = static_cast<double*>(at(o_csc_val));
     int* csr_start = static_cast<int*>(at(o_csr_start));
     int* csr_col = static_cast<int*>(at(o_csr_col));
@@ -395,9 +468,13 @@ int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* 
     // ---- uploads
     CU(cudaEventRecord(ctx.ev_a, s));
     const cudaMemcpyKind in_kind = dev_in ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    CU(cudaMemcpyAsync(at(o_csc_start), lp->col_start, sizeof(int) * (size_t)(n + 1), in_kind, s));
+    if (nnz) CU(cudaMemcpyAsync(at(o_csc_row), lp->row_index, sizeof(int) * (size_t)nnz, in_kind, s));
+    CU(cudaMemsetAsync(static_cast<int*>(at(o_csc_row)) + nnz, 0, sizeof(int) * 16, s));
+    CU(cudaMemsetAsync(static_cast<double*>(at(o_csc_val)) + nnz, 0, sizeof(double) * 16, s));
+    CU(cudaMemsetAsync(static_cast<int*>(at(o_csr_col)) + nnz, 0, sizeof(int) * 16, s));
+    CU(cudaMemsetAsync(static_cast<double*>(at(o_csr_val)) + nnz, 0, sizeof(double) * 16, s));
     if (!dev_in) {
-        CU(cudaMemcpyAsync(at(o_csc_start), lp->col_start, sizeof(int) * (size_t)(n + 1), in_kind, s));
-        if (nnz) CU(cudaMemcpyAsync(at(o_csc_row), lp->row_index, sizeof(int) * (size_t)nnz, in_kind, s));
         CU(cudaMemcpyAsync(at(o_in_obj), lp->objective, sizeof(double) * (size_t)n, in_kind, s));
         CU(cudaMemcpyAsync(at(o_in_lo), lp->var_lower, sizeof(double) * (size_t)n, in_kind, s));
         CU(cudaMemcpyAsync(at(o_in_hi), lp->var_upper, sizeof(double) * (size_t)n, in_kind, s));
@@ -481,7 +558,10 @@ int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* 
                 static_cast<double*>(at(o_tr[1])), static_cast<double*>(at(o_tr[2])),
                 static_cast<double*>(at(o_tr[3])), static_cast<double*>(at(o_tr[4])),
                 static_cast<int*>(at(o_tr_rs))};
-    const Plan pl = make_plan(ctx, m, n, nnz);
+    const Plan pl = make_plan<double>(ctx, m, n, nnz, o->lanes_per_column, o->lanes_per_row,
+                                      static_cast<int*>(at(o_col_bounds)), static_cast<int*>(at(o_row_bounds)));
+    TRY(build_tiles(ctx, pl, m, n, csc_start, csr_start, static_cast<int*>(at(o_col_bounds)),
+                    static_cast<int*>(at(o_row_bounds)), chunk));
 
     // ---- PDHG loop in restart chunks
     const long long R = o->restart_every;

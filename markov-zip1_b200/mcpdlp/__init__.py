@@ -82,6 +82,8 @@ class PdlpOptions:
     refine_max_rounds: int = 12
     refine_inner_tolerance: float = 1e-4
     check_every_chunks: int = 1
+    lanes_per_column: int = 0                      # SpMV tuning, 0 = chosen by line length
+    lanes_per_row: int = 0
     initial_primal: Optional[np.ndarray] = None   # warm start, original space
     initial_dual: Optional[np.ndarray] = None
 

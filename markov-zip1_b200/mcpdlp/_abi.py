@@ -82,7 +82,9 @@ class McPdlpOptions(C.Structure):
         ("refine_max_rounds", C.c_int32),
         ("refine_inner_tolerance", C.c_double),
         ("check_every_chunks", C.c_int32),
-        ("reserved_i", C.c_int32 * 7),
+        ("lanes_per_column", C.c_int32),
+        ("lanes_per_row", C.c_int32),
+        ("reserved_i", C.c_int32 * 5),
         ("reserved_d", C.c_double * 8),
     ]
 
