@@ -240,6 +240,28 @@ int mc_ruiz_equilibrate(mc_pdlp_ctx* ctx, int32_t m, int32_t n, int64_t nnz,
                         double* row_lower, double* row_upper, int64_t max_iterations,
                         double* row_scale, double* col_scale, int64_t* iterations_executed);
 
+/*
+ * mc_ruiz_equilibrate_noalloc: the same equilibration as mc_ruiz_equilibrate,
+ * with bit-identical results, for callers that cannot allocate device memory
+ * (work inside CUDA stream capture, device memory owned by another allocator,
+ * a request path that must not allocate).  No counterpart in the reference.
+ * It allocates nothing: its working memory is one static device array of
+ * about 8 MiB that every GPU loading the library holds until exit.
+ * Limits: m + n <= 1,048,576, else MC_ERR_RESOURCE_LIMIT (nothing launched).
+ * Runs on the current device and `stream` (a cudaStream_t, NULL = default
+ * stream); *iterations_executed (may be NULL) is read back with a stream
+ * synchronisation.  The first call on a device looks the array up with
+ * cudaGetSymbolAddress: make it before any stream capture.  Calls share the
+ * array, so calls that can overlap on the GPU race and must be serialised.
+ */
+int mc_ruiz_equilibrate_noalloc(int32_t m, int32_t n, int64_t nnz, const int32_t* col_start,
+                                const int32_t* row_index, double* csc_value,
+                                const int32_t* row_start, const int32_t* col_index,
+                                double* csr_value, double* objective, double* var_lower,
+                                double* var_upper, double* row_lower, double* row_upper,
+                                int64_t max_iterations, double* row_scale, double* col_scale,
+                                int64_t* iterations_executed, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

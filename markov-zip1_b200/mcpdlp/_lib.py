@@ -56,6 +56,8 @@ ENGINE_SIGNATURES = {
     "mc_csc_to_csr": ([_VP, _I32, _I32, _I64, _VP, _VP, _VP, _VP, _VP, _VP], C.c_int),
     "mc_ruiz_equilibrate": ([_VP, _I32, _I32, _I64, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP,
                              _VP, _VP, _VP, _I64, _VP, _VP, _VP], C.c_int),
+    "mc_ruiz_equilibrate_noalloc": ([_I32, _I32, _I64, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP,
+                                     _VP, _VP, _VP, _I64, _VP, _VP, _VP, _VP], C.c_int),
 }
 
 
