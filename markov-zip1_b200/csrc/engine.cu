@@ -179,11 +179,6 @@ int pick_lanes(double mean_len) {
     return g;
 }
 
-int solve_fp32_refine(Ctx&, const mc_lp*, const mc_pdlp_options*, const double*, const double*,
-                      double*, double*, mc_pdlp_result*, mc_pdlp_trace*) {
-    return set_error(MC_ERR_INVALID_ARGUMENT, "MC_PRECISION_FP32_REFINE is not available in this build");
-}
-
 }  // namespace mc
 
 #include "solve.cuh"

@@ -124,10 +124,6 @@ int grid_for(const Ctx& ctx, K kernel, long long work_items, int per_block, size
 }
 int pick_lanes(double mean_len);
 
-int solve_fp32_refine(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* warm_x,
-                      const double* warm_y, double* x_out, double* y_out, mc_pdlp_result* res,
-                      mc_pdlp_trace* trace);
-
 int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* warm_x,
              const double* warm_y, double* x_out, double* y_out, mc_pdlp_result* res,
              mc_pdlp_trace* trace);

@@ -103,24 +103,36 @@ __device__ __forceinline__ T line_dot(const int* __restrict__ start, const int* 
     return group_sum<G>((s0 + s1) + (s2 + s3));
 }
 
-// Two dots of the same line (A x-bar and A dx on step-size iterations).
+// Two dots of the same line (A x-bar and A dx on step-size iterations), two
+// entries per lane per step, both vectors gathered with the keep policy.
 template <int G, class T>
 __device__ __forceinline__ void line_dot2(const int* __restrict__ start, const int* __restrict__ idx,
                                           const T* __restrict__ val, const T* __restrict__ v,
                                           const T* __restrict__ w, int j, bool valid, int sub,
                                           T& out_v, T& out_w, unsigned long long pol) {
-    T sv = T(0), sw = T(0);
+    T sv0 = T(0), sw0 = T(0), sv1 = T(0), sw1 = T(0);
     if (valid) {
         const int b = __ldg(start + j), e = __ldg(start + j + 1);
-        for (int p = b + sub; p < e; p += G) {
-            const int i = ld_stream(idx + p);
-            const T a = ld_stream(val + p);
-            sv = fma(a, ld_keep(v + i, pol), sv);
-            sw = fma(a, __ldg(w + i), sw);
+        int p = b + sub;
+        for (; p + G < e; p += 2 * G) {
+            const int i0 = ld_stream(idx + p), i1 = ld_stream(idx + p + G);
+            const T a0 = ld_stream(val + p), a1 = ld_stream(val + p + G);
+            const T v0 = ld_keep(v + i0, pol), v1 = ld_keep(v + i1, pol);
+            const T w0 = ld_keep(w + i0, pol), w1 = ld_keep(w + i1, pol);
+            sv0 = fma(a0, v0, sv0);
+            sw0 = fma(a0, w0, sw0);
+            sv1 = fma(a1, v1, sv1);
+            sw1 = fma(a1, w1, sw1);
+        }
+        if (p < e) {
+            const int i0 = ld_stream(idx + p);
+            const T a0 = ld_stream(val + p);
+            sv0 = fma(a0, ld_keep(v + i0, pol), sv0);
+            sw0 = fma(a0, ld_keep(w + i0, pol), sw0);
         }
     }
-    out_v = group_sum<G>(sv);
-    out_w = group_sum<G>(sw);
+    out_v = group_sum<G>(sv0 + sv1);
+    out_w = group_sum<G>(sw0 + sw1);
 }
 
 // Plain y = A x over a compressed-row matrix (kernel-level entry point).
@@ -301,10 +313,71 @@ __global__ void __launch_bounds__(kBlock) k_dual_apply(Iterates<T> P, int k) {
 }
 
 // --------------------------------------------------------------- residuals
-// compute_unscaled_residuals (pdlp.cpp:62-135) over the averages, row part:
-// (A x_avg)_i unscaled, relative row violation (max), row part of the dual
-// objective (sum).  Always FP64 (the FP32 engine evaluates its FP32 averages
-// through double gathers).
+// compute_unscaled_residuals (pdlp.cpp:62-135) over the averages.  The row and
+// column terms are shared by the FP64 kernels below and the mixed-precision
+// kernels (mixed.cuh), which evaluate the same formulas on base + correction.
+
+// Row i: s = (A x_avg)_i in the scaled space, y_avg_i scaled.
+struct RowTerms {
+    double vmax = 0.0, dsum = 0.0, bad = 0.0;
+    __device__ __forceinline__ void add(const Original& O, int i, double s, double y_scaled) {
+        const double ax = __ddiv_rn(s, O.row_scale[i]);
+        const double lo = O.blo[i], hi = O.bhi[i];
+        const double proj = clampv(ax, lo, hi);
+        const double r = fabs(ax - proj);
+        const double sc = 1.0 + maxv(fabs(ax), fabs(proj) < 1e299 ? fabs(proj) : 0.0);
+        vmax = maxv(vmax, r / sc);
+        const double yu = __dmul_rn(y_scaled, O.row_scale[i]);
+        if (yu > 0.0 && hi < 1e299) dsum -= __dmul_rn(yu, hi);
+        else if (yu < 0.0 && lo > -1e299) dsum -= __dmul_rn(yu, lo);
+        if (!isfinite(ax) || !isfinite(yu)) bad += 1.0;
+    }
+    __device__ __forceinline__ void store(double* partials, double* scratch) {
+        vmax = block_reduce(vmax, scratch, OpMax());
+        if (threadIdx.x == 0) partials[SLOT_ROW_MAX * kMaxPartials + blockIdx.x] = vmax;
+        dsum = block_reduce(dsum, scratch, OpSum());
+        if (threadIdx.x == 0) partials[SLOT_ROW_DOBJ * kMaxPartials + blockIdx.x] = dsum;
+        bad = block_reduce(bad, scratch, OpSum());
+        if (threadIdx.x == 0) partials[SLOT_NAN * kMaxPartials + blockIdx.x] = bad;
+    }
+};
+
+// Column j: s = (A^T y_avg)_j in the scaled space, x_avg_j scaled.
+struct ColTerms {
+    double vmax = 0.0, dres = 0.0, pobj = 0.0, dobj = 0.0, bad = 0.0;
+    __device__ __forceinline__ void add(const Original& O, int j, double s, double x_scaled) {
+        const double aty = __ddiv_rn(s, O.col_scale[j]);
+        const double xu = __dmul_rn(x_scaled, O.col_scale[j]);
+        const double lo = O.lo[j], hi = O.hi[j];
+        const double proj = clampv(xu, lo, hi);
+        const double r = fabs(xu - proj);
+        const double sc = 1.0 + maxv(fabs(xu), fabs(proj) < 1e299 ? fabs(proj) : 0.0);
+        vmax = maxv(vmax, r / sc);
+        const double g = __dadd_rn(O.c[j], aty);
+        const double xp = clampv(__dsub_rn(xu, g), lo, hi);
+        const double diff = __dsub_rn(xu, xp);
+        dres += __dmul_rn(diff, diff);
+        pobj += __dmul_rn(O.obj[j], xu);
+        if (g > 0.0 && lo > -1e299) dobj += __dmul_rn(g, lo);
+        else if (g < 0.0 && hi < 1e299) dobj += __dmul_rn(g, hi);
+        if (!isfinite(xu) || !isfinite(g)) bad += 1.0;
+    }
+    __device__ __forceinline__ void store(double* partials, double* scratch) {
+        vmax = block_reduce(vmax, scratch, OpMax());
+        if (threadIdx.x == 0) partials[SLOT_COL_MAX * kMaxPartials + blockIdx.x] = vmax;
+        dres = block_reduce(dres, scratch, OpSum());
+        if (threadIdx.x == 0) partials[SLOT_COL_DRES * kMaxPartials + blockIdx.x] = dres;
+        pobj = block_reduce(pobj, scratch, OpSum());
+        if (threadIdx.x == 0) partials[SLOT_COL_POBJ * kMaxPartials + blockIdx.x] = pobj;
+        dobj = block_reduce(dobj, scratch, OpSum());
+        if (threadIdx.x == 0) partials[SLOT_COL_DOBJ * kMaxPartials + blockIdx.x] = dobj;
+        bad = block_reduce(bad, scratch, OpSum());
+        if (threadIdx.x == 0) partials[SLOT_NAN * kMaxPartials + kMaxPartials / 2 + blockIdx.x] = bad;
+    }
+};
+
+// Row part: (A x_avg)_i unscaled, relative row violation (max), row part of
+// the dual objective (sum).
 template <int G, class T>
 __global__ void __launch_bounds__(kBlock) k_residual_rows(Iterates<T> P, Original O) {
     __shared__ double scratch[32];
@@ -314,7 +387,7 @@ __global__ void __launch_bounds__(kBlock) k_residual_rows(Iterates<T> P, Origina
     const int lane = threadIdx.x & 31, sub = lane % G, slot = lane / G;
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    double vmax = 0.0, dsum = 0.0, bad = 0.0;
+    RowTerms acc;
     for (long long t = warp; t * LPW < P.m; t += nwarps) {
         const int i = (int)(t * LPW) + slot;
         const bool valid = i < P.m;
@@ -325,25 +398,9 @@ __global__ void __launch_bounds__(kBlock) k_residual_rows(Iterates<T> P, Origina
                 s = fma((double)P.csr_val[p], (double)P.x_avg[P.csr_col[p]], s);
         }
         s = group_sum<G>(s);
-        if (valid && sub == 0) {
-            const double ax = __ddiv_rn(s, O.row_scale[i]);
-            const double lo = O.blo[i], hi = O.bhi[i];
-            const double proj = clampv(ax, lo, hi);
-            const double r = fabs(ax - proj);
-            const double sc = 1.0 + maxv(fabs(ax), fabs(proj) < 1e299 ? fabs(proj) : 0.0);
-            vmax = maxv(vmax, r / sc);
-            const double yu = __dmul_rn((double)P.y_avg[i], O.row_scale[i]);
-            if (yu > 0.0 && hi < 1e299) dsum -= __dmul_rn(yu, hi);
-            else if (yu < 0.0 && lo > -1e299) dsum -= __dmul_rn(yu, lo);
-            if (!isfinite(ax) || !isfinite(yu)) bad += 1.0;
-        }
+        if (valid && sub == 0) acc.add(O, i, s, (double)P.y_avg[i]);
     }
-    vmax = block_reduce(vmax, scratch, OpMax());
-    if (threadIdx.x == 0) P.partials[SLOT_ROW_MAX * kMaxPartials + blockIdx.x] = vmax;
-    dsum = block_reduce(dsum, scratch, OpSum());
-    if (threadIdx.x == 0) P.partials[SLOT_ROW_DOBJ * kMaxPartials + blockIdx.x] = dsum;
-    bad = block_reduce(bad, scratch, OpSum());
-    if (threadIdx.x == 0) P.partials[SLOT_NAN * kMaxPartials + blockIdx.x] = bad;
+    acc.store(P.partials, scratch);
 }
 
 // Column part: (A^T y_avg)_j unscaled, bound violation (max), squared dual
@@ -357,7 +414,7 @@ __global__ void __launch_bounds__(kBlock) k_residual_cols(Iterates<T> P, Origina
     const int lane = threadIdx.x & 31, sub = lane % G, slot = lane / G;
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    double vmax = 0.0, dres = 0.0, pobj = 0.0, dobj = 0.0, bad = 0.0;
+    ColTerms acc;
     for (long long t = warp; t * LPW < P.n; t += nwarps) {
         const int j = (int)(t * LPW) + slot;
         const bool valid = j < P.n;
@@ -368,34 +425,9 @@ __global__ void __launch_bounds__(kBlock) k_residual_cols(Iterates<T> P, Origina
                 s = fma((double)P.csc_val[p], (double)P.y_avg[P.csc_row[p]], s);
         }
         s = group_sum<G>(s);
-        if (valid && sub == 0) {
-            const double aty = __ddiv_rn(s, O.col_scale[j]);
-            const double xu = __dmul_rn((double)P.x_avg[j], O.col_scale[j]);
-            const double lo = O.lo[j], hi = O.hi[j];
-            const double proj = clampv(xu, lo, hi);
-            const double r = fabs(xu - proj);
-            const double sc = 1.0 + maxv(fabs(xu), fabs(proj) < 1e299 ? fabs(proj) : 0.0);
-            vmax = maxv(vmax, r / sc);
-            const double g = __dadd_rn(O.c[j], aty);
-            const double xp = clampv(__dsub_rn(xu, g), lo, hi);
-            const double diff = __dsub_rn(xu, xp);
-            dres += __dmul_rn(diff, diff);
-            pobj += __dmul_rn(O.obj[j], xu);
-            if (g > 0.0 && lo > -1e299) dobj += __dmul_rn(g, lo);
-            else if (g < 0.0 && hi < 1e299) dobj += __dmul_rn(g, hi);
-            if (!isfinite(xu) || !isfinite(g)) bad += 1.0;
-        }
+        if (valid && sub == 0) acc.add(O, j, s, (double)P.x_avg[j]);
     }
-    vmax = block_reduce(vmax, scratch, OpMax());
-    if (threadIdx.x == 0) P.partials[SLOT_COL_MAX * kMaxPartials + blockIdx.x] = vmax;
-    dres = block_reduce(dres, scratch, OpSum());
-    if (threadIdx.x == 0) P.partials[SLOT_COL_DRES * kMaxPartials + blockIdx.x] = dres;
-    pobj = block_reduce(pobj, scratch, OpSum());
-    if (threadIdx.x == 0) P.partials[SLOT_COL_POBJ * kMaxPartials + blockIdx.x] = pobj;
-    dobj = block_reduce(dobj, scratch, OpSum());
-    if (threadIdx.x == 0) P.partials[SLOT_COL_DOBJ * kMaxPartials + blockIdx.x] = dobj;
-    bad = block_reduce(bad, scratch, OpSum());
-    if (threadIdx.x == 0) P.partials[(SLOT_NAN + 0) * kMaxPartials + kMaxPartials / 2 + blockIdx.x] = bad;
+    acc.store(P.partials, scratch);
 }
 
 // Device trace of the restart checks (optional).

@@ -5,6 +5,7 @@
 #include "iter_kernels.cuh"
 #include "setup_kernels.cuh"
 #include "staged.cuh"
+#include "mixed.cuh"
 
 #include <cmath>
 #include <cstring>
@@ -211,85 +212,159 @@ int ruiz(Ctx& ctx, int m, int n, long long nnz, const int* csc_start, const int*
 }
 
 // ------------------------------------------------------- iteration chunks
-template <class T>
-int enqueue_iteration(Ctx& ctx, const Iterates<T>& P, const Plan& pl, int k, bool step, const Controls& ctl) {
-    cudaStream_t s = ctx.stream;
-    const size_t sm = staged_smem_bytes<T>();
-    ctx.begin_launch(MC_KERNEL_PRIMAL);
-    if (pl.staged_col) {
-        if (step) k_primal_staged<true, T><<<pl.nb_col_step, kBlock, sm, s>>>(P, pl.tiles, k);
-        else k_primal_staged<false, T><<<pl.nb_col, kBlock, sm, s>>>(P, pl.tiles, k);
-    } else if (step) {
-        MC_DISPATCH_G(pl.g_col, (k_primal<G, true, T><<<pl.nb_col_step, kBlock, 0, s>>>(P, k)));
-    } else {
-        MC_DISPATCH_G(pl.g_col, (k_primal<G, false, T><<<pl.nb_col, kBlock, 0, s>>>(P, k)));
-    }
-    ctx.end_launch();
-    if (step) {
-        ctx.begin_launch(MC_KERNEL_DUAL_STEP);
-        if (pl.staged_row) k_dual_probe_staged<T><<<pl.nb_row_step, kBlock, sm, s>>>(P, pl.tiles);
-        else MC_DISPATCH_G(pl.g_row, (k_dual_probe<G, T><<<pl.nb_row_step, kBlock, 0, s>>>(P)));
-        ctx.end_launch();
-        ctx.begin_launch(MC_KERNEL_OTHER);
-        k_step_size<<<1, 1024, 0, s>>>(P.partials, pl.nb_col_step, pl.nb_row_step, P.st, ctl);
-        ctx.end_launch();
-        ctx.begin_launch(MC_KERNEL_DUAL_STEP);
-        k_dual_apply<T><<<pl.nb_m, kBlock, 0, s>>>(P, k);
-        ctx.end_launch();
-    } else {
-        ctx.begin_launch(MC_KERNEL_DUAL);
-        if (pl.staged_row) k_dual_staged<T><<<pl.nb_row, kBlock, sm, s>>>(P, pl.tiles, k);
-        else MC_DISPATCH_G(pl.g_row, (k_dual<G, T><<<pl.nb_row, kBlock, 0, s>>>(P, k)));
-        ctx.end_launch();
-    }
-    return ctx.launch_check("iteration");
-}
+// One precision's way of enqueuing iterations and restart checks.  FP64 runs
+// the fused kernels on the iterate itself; the mixed form runs the FP32
+// kernels on the correction and checks in FP64 (mixed.cuh).
+struct Engine64 {
+    Iterates<double> P;
+    Original O;
+    Plan pl;
 
-template <class T>
-int enqueue_check(Ctx& ctx, const Iterates<T>& P, const Original& O, const Plan& pl, long long span,
-                  int final_pass, const Controls& ctl, const TraceBuf& tr) {
-    cudaStream_t s = ctx.stream;
-    ctx.begin_launch(MC_KERNEL_RESIDUAL);
-    MC_DISPATCH_G(pl.g_row, (k_residual_rows<G, T><<<pl.nb_res_row, kBlock, 0, s>>>(P, O)));
-    ctx.end_launch();
-    ctx.begin_launch(MC_KERNEL_RESIDUAL);
-    MC_DISPATCH_G(pl.g_col, (k_residual_cols<G, T><<<pl.nb_res_col, kBlock, 0, s>>>(P, O)));
-    ctx.end_launch();
-    ctx.begin_launch(MC_KERNEL_RESIDUAL);
-    k_finalize<<<1, 1024, 0, s>>>(P.partials, pl.nb_res_row, pl.nb_res_col, span, final_pass, O.offset, ctl, tr, P.st);
-    ctx.end_launch();
-    if (!final_pass) {
-        ctx.begin_launch(MC_KERNEL_OTHER);
-        k_restart_copy<T><<<pl.nb_nm, kBlock, 0, s>>>(P);
+    int iteration(Ctx& ctx, int k, bool step, const Controls& ctl) const {
+        cudaStream_t s = ctx.stream;
+        const size_t sm = staged_smem_bytes<double>();
+        ctx.begin_launch(MC_KERNEL_PRIMAL);
+        if (pl.staged_col) {
+            if (step) k_primal_staged<true, double><<<pl.nb_col_step, kBlock, sm, s>>>(P, pl.tiles, k);
+            else k_primal_staged<false, double><<<pl.nb_col, kBlock, sm, s>>>(P, pl.tiles, k);
+        } else if (step) {
+            MC_DISPATCH_G(pl.g_col, (k_primal<G, true, double><<<pl.nb_col_step, kBlock, 0, s>>>(P, k)));
+        } else {
+            MC_DISPATCH_G(pl.g_col, (k_primal<G, false, double><<<pl.nb_col, kBlock, 0, s>>>(P, k)));
+        }
         ctx.end_launch();
+        if (step) {
+            ctx.begin_launch(MC_KERNEL_DUAL_STEP);
+            if (pl.staged_row) {
+                k_dual_probe_staged<double><<<pl.nb_row_step, kBlock, sm, s>>>(P, pl.tiles);
+            } else {
+                MC_DISPATCH_G(pl.g_row, (k_dual_probe<G, double><<<pl.nb_row_step, kBlock, 0, s>>>(P)));
+            }
+            ctx.end_launch();
+            ctx.begin_launch(MC_KERNEL_OTHER);
+            k_step_size<<<1, 1024, 0, s>>>(P.partials, pl.nb_col_step, pl.nb_row_step, P.st, ctl);
+            ctx.end_launch();
+            ctx.begin_launch(MC_KERNEL_DUAL_STEP);
+            k_dual_apply<double><<<pl.nb_m, kBlock, 0, s>>>(P, k);
+            ctx.end_launch();
+        } else {
+            ctx.begin_launch(MC_KERNEL_DUAL);
+            if (pl.staged_row) {
+                k_dual_staged<double><<<pl.nb_row, kBlock, sm, s>>>(P, pl.tiles, k);
+            } else {
+                MC_DISPATCH_G(pl.g_row, (k_dual<G, double><<<pl.nb_row, kBlock, 0, s>>>(P, k)));
+            }
+            ctx.end_launch();
+        }
+        return ctx.launch_check("iteration");
     }
-    return ctx.launch_check("check");
-}
+
+    int check(Ctx& ctx, long long span, int final_pass, const Controls& ctl, const TraceBuf& tr) const {
+        cudaStream_t s = ctx.stream;
+        ctx.begin_launch(MC_KERNEL_RESIDUAL);
+        MC_DISPATCH_G(pl.g_row, (k_residual_rows<G, double><<<pl.nb_res_row, kBlock, 0, s>>>(P, O)));
+        ctx.end_launch();
+        ctx.begin_launch(MC_KERNEL_RESIDUAL);
+        MC_DISPATCH_G(pl.g_col, (k_residual_cols<G, double><<<pl.nb_res_col, kBlock, 0, s>>>(P, O)));
+        ctx.end_launch();
+        ctx.begin_launch(MC_KERNEL_RESIDUAL);
+        k_finalize<<<1, 1024, 0, s>>>(P.partials, pl.nb_res_row, pl.nb_res_col, span, final_pass, O.offset, ctl, tr,
+                                      P.st);
+        ctx.end_launch();
+        if (!final_pass) {
+            ctx.begin_launch(MC_KERNEL_OTHER);
+            k_restart_copy<double><<<pl.nb_nm, kBlock, 0, s>>>(P);
+            ctx.end_launch();
+        }
+        return ctx.launch_check("check");
+    }
+};
+
+struct EngineMixed {
+    Iterates<float> P;
+    MixedState M;
+    Original O;
+    Plan pl;
+    int nb_res_row = 1, nb_res_col = 1, nb_recenter = 1, nb_apply = 1;
+
+    int iteration(Ctx& ctx, int k, bool step, const Controls& ctl) const {
+        cudaStream_t s = ctx.stream;
+        ctx.begin_launch(MC_KERNEL_PRIMAL);
+        if (step) {
+            MC_DISPATCH_G(pl.g_col, (k_primal<G, true, float><<<pl.nb_col_step, kBlock, 0, s>>>(P, k)));
+        } else {
+            MC_DISPATCH_G(pl.g_col, (k_primal<G, false, float><<<pl.nb_col, kBlock, 0, s>>>(P, k)));
+        }
+        ctx.end_launch();
+        if (step) {
+            ctx.begin_launch(MC_KERNEL_DUAL_STEP);
+            MC_DISPATCH_G(pl.g_row, (k_dual_probe<G, float><<<pl.nb_row_step, kBlock, 0, s>>>(P)));
+            ctx.end_launch();
+            ctx.begin_launch(MC_KERNEL_OTHER);
+            k_step_size<<<1, 1024, 0, s>>>(P.partials, pl.nb_col_step, pl.nb_row_step, P.st, ctl);
+            ctx.end_launch();
+            ctx.begin_launch(MC_KERNEL_DUAL_STEP);
+            k_dual_apply_mx<<<nb_apply, kBlock, 0, s>>>(P, M, k);
+            ctx.end_launch();
+        } else {
+            ctx.begin_launch(MC_KERNEL_DUAL);
+            MC_DISPATCH_G(pl.g_row, (k_dual_mx<G><<<pl.nb_row, kBlock, 0, s>>>(P, M, k)));
+            ctx.end_launch();
+        }
+        return ctx.launch_check("iteration (mixed)");
+    }
+
+    int residual_pass(Ctx& ctx) const {
+        cudaStream_t s = ctx.stream;
+        ctx.begin_launch(MC_KERNEL_RESIDUAL);
+        MC_DISPATCH_G(pl.g_row, (k_residual_rows_mx<G><<<nb_res_row, kBlock, 0, s>>>(P, M, O)));
+        ctx.end_launch();
+        ctx.begin_launch(MC_KERNEL_RESIDUAL);
+        MC_DISPATCH_G(pl.g_col, (k_residual_cols_mx<G><<<nb_res_col, kBlock, 0, s>>>(P, M, O)));
+        ctx.end_launch();
+        return ctx.launch_check("residual (mixed)");
+    }
+
+    int recenter(Ctx& ctx, int force) const {
+        ctx.begin_launch(MC_KERNEL_OTHER);
+        k_recenter_mx<<<nb_recenter, kBlock, 0, ctx.stream>>>(P, M, force);
+        ctx.end_launch();
+        return ctx.launch_check("recenter (mixed)");
+    }
+
+    int check(Ctx& ctx, long long span, int final_pass, const Controls& ctl, const TraceBuf& tr) const {
+        TRY(residual_pass(ctx));
+        ctx.begin_launch(MC_KERNEL_RESIDUAL);
+        k_finalize<<<1, 1024, 0, ctx.stream>>>(P.partials, nb_res_row, nb_res_col, span, final_pass, O.offset, ctl,
+                                               tr, P.st);
+        ctx.end_launch();
+        if (!final_pass) TRY(recenter(ctx, 0));
+        return ctx.launch_check("check (mixed)");
+    }
+};
 
 // iterations [k0, k1) of the chunk that starts at global iteration `base`
-template <class T>
-int enqueue_span(Ctx& ctx, const Iterates<T>& P, const Plan& pl, long long base, int k0, int k1,
-                 const Controls& ctl) {
+template <class E>
+int enqueue_span(Ctx& ctx, const E& eng, long long base, int k0, int k1, const Controls& ctl) {
     for (int k = k0; k < k1; ++k) {
         const bool step = ctl.adaptive_step && ((base + k) % 10 == 0);
-        TRY(enqueue_iteration(ctx, P, pl, k, step, ctl));
+        TRY(eng.iteration(ctx, k, step, ctl));
     }
     return MC_OK;
 }
 
 // Capture one full chunk (restart_every iterations + check) as a graph; the
 // schedule of step-size iterations depends only on base % 10.
-template <class T>
-int chunk_graph(Ctx& ctx, const Iterates<T>& P, const Original& O, const Plan& pl, long long base,
-                long long R, const Controls& ctl, const TraceBuf& tr, cudaGraphExec_t* out,
-                long long recipe[MC_KERNEL_KINDS]) {
+template <class E>
+int chunk_graph(Ctx& ctx, const E& eng, long long base, long long R, const Controls& ctl, const TraceBuf& tr,
+                cudaGraphExec_t* out, long long recipe[MC_KERNEL_KINDS]) {
     const int key = (int)(base % 10);
     long long before[MC_KERNEL_KINDS];
     std::memcpy(before, ctx.launches, sizeof before);
     CU(cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeThreadLocal));
     ctx.capturing = true;
-    int rc = enqueue_span(ctx, P, pl, base, 0, (int)R, ctl);
-    if (rc == MC_OK) rc = enqueue_check(ctx, P, O, pl, R, 0, ctl, tr);
+    int rc = enqueue_span(ctx, eng, base, 0, (int)R, ctl);
+    if (rc == MC_OK) rc = eng.check(ctx, R, 0, ctl, tr);
     ctx.capturing = false;
     cudaGraph_t g = nullptr;
     const cudaError_t e = cudaStreamEndCapture(ctx.stream, &g);
@@ -308,6 +383,69 @@ int chunk_graph(Ctx& ctx, const Iterates<T>& P, const Original& O, const Plan& p
     if (e2 != cudaSuccess) return cuda_fail(e2, "cudaGraphInstantiate", __LINE__);
     ctx.graphs[key] = exec;
     *out = exec;
+    return MC_OK;
+}
+
+// The PDHG loop (pdlp.cpp:194-275) in restart chunks, each a CUDA graph
+// replay; the host polls the device state one chunk group behind.  Returns
+// with the stream synchronised.
+template <class E>
+int run_chunks(Ctx& ctx, const E& eng, DevState* st, long long maxit, long long R, int poll_every,
+               const Controls& ctl, const TraceBuf& tr) {
+    cudaStream_t s = ctx.stream;
+    ctx.release_graphs();
+    const long long full_chunks = maxit / R;
+    long long base = 0;
+    bool done = false;
+    long long recipe[10][MC_KERNEL_KINDS] = {};
+    int inflight = 0;
+    int ev_idx = 0;
+    bool have_prev = false;
+    for (long long chunk = 0; chunk < full_chunks && !done; ++chunk) {
+        if (ctx.profiling) {
+            TRY(enqueue_span(ctx, eng, base, 0, (int)R, ctl));
+            TRY(eng.check(ctx, R, 0, ctl, tr));
+            TRY(ctx.drain_profile());
+        } else {
+            const int key = (int)(base % 10);
+            auto it = ctx.graphs.find(key);
+            cudaGraphExec_t exec = nullptr;
+            if (it == ctx.graphs.end()) {
+                TRY(chunk_graph(ctx, eng, base, R, ctl, tr, &exec, recipe[key]));
+            } else {
+                exec = it->second;
+            }
+            CU(cudaGraphLaunch(exec, s));
+            for (int q = 0; q < MC_KERNEL_KINDS; ++q) ctx.launches[q] += recipe[key][q];
+        }
+        base += R;
+        ++inflight;
+        if (inflight >= poll_every || chunk + 1 == full_chunks) {
+            if (have_prev) {
+                CU(cudaEventSynchronize(ctx.ev_poll[ev_idx ^ 1]));
+                if (ctx.h_state[ev_idx ^ 1].done) done = true;
+            }
+            CU(cudaMemcpyAsync(&ctx.h_state[ev_idx], st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
+            CU(cudaEventRecord(ctx.ev_poll[ev_idx], s));
+            have_prev = true;
+            ev_idx ^= 1;
+            inflight = 0;
+        }
+    }
+    CU(cudaStreamSynchronize(s));
+    CU(cudaMemcpy(&ctx.h_state[2], st, sizeof(DevState), cudaMemcpyDeviceToHost));
+    if (!ctx.h_state[2].done) {
+        // the loop ran out: remaining partial chunk, then the final evaluation
+        // (pdlp.cpp:263-265); after a whole number of chunks the last check
+        // already holds the averages' residuals
+        const long long rem = maxit - full_chunks * R;
+        if (rem > 0 || full_chunks == 0) {
+            TRY(enqueue_span(ctx, eng, base, 0, (int)rem, ctl));
+            TRY(eng.check(ctx, rem, 1, ctl, tr));
+            TRY(ctx.drain_profile());
+        }
+    }
+    CU(cudaStreamSynchronize(s));
     return MC_OK;
 }
 
@@ -333,6 +471,8 @@ int validate_options(const mc_pdlp_options* o) {
     if ((o->lanes_per_column && o->lanes_per_column != -1 && !valid_lanes(o->lanes_per_column)) ||
         (o->lanes_per_row && o->lanes_per_row != -1 && !valid_lanes(o->lanes_per_row)))
         return set_error(MC_ERR_INVALID_ARGUMENT, "lanes per line must be 0, -1 or a power of two <= 32");
+    if (o->precision == MC_PRECISION_FP32_REFINE && (o->lanes_per_column == -1 || o->lanes_per_row == -1))
+        return set_error(MC_ERR_INVALID_ARGUMENT, "the staged kernels are FP64 only");
     return MC_OK;
 }
 
@@ -366,7 +506,6 @@ int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* 
     if (trace) trace->count = 0;
     TRY(validate_options(o));
     TRY(validate_lp(lp));
-    if (o->precision == MC_PRECISION_FP32_REFINE) return solve_fp32_refine(ctx, lp, o, warm_x, warm_y, x_out, y_out, res, trace);
     const int m = lp->num_rows, n = lp->num_cols;
     const long long nnz = lp->nnz;
     if (m == 0 || n == 0) {  // pdlp.cpp:144-149
@@ -376,6 +515,7 @@ int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* 
         res->total_ms = now_ms() - t_begin;
         return MC_OK;
     }
+    const bool mixed = o->precision == MC_PRECISION_FP32_REFINE;
     const bool dev_in = lp->memory == MC_MEMORY_DEVICE;
     cudaStream_t s = ctx.stream;
     for (int q = 0; q < MC_KERNEL_KINDS; ++q) {
@@ -422,6 +562,14 @@ int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* 
     size_t o_tr[5];
     for (auto& v : o_tr) v = L.add<double>(trace_cap);
     const size_t o_tr_rs = L.add<int>(trace_cap);
+    // mixed form: FP32 matrix copies, FP32 correction iterates and cycle data
+    size_t o_f_cscv = 0, o_f_csrv = 0, o_fn[9] = {}, o_fm[8] = {};
+    if (mixed) {
+        o_f_cscv = L.add<float>(nnz + 16);
+        o_f_csrv = L.add<float>(nnz + 16);
+        for (auto& v : o_fn) v = L.add<float>(n);
+        for (auto& v : o_fm) v = L.add<float>(m);
+    }
     TRY(ctx.arena.reserve(L.offset));
     char* A = static_cast<char*>(ctx.arena.base);
     auto at = [&](size_t off) { return static_cast<void*>(A + off); };
@@ -503,7 +651,7 @@ int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* 
                          (bad & 8) ? "zero or non-finite value" : "");
     }
 
-    // ---- setup
+    // ---- setup (FP64, both forms)
     CU(cudaMemsetAsync(st, 0, sizeof(DevState), s));
     TRY(build_csr(ctx, m, n, nnz, csc_start, csc_row, csc_val, csr_start, csr_col, csr_val,
                   static_cast<int*>(at(o_cursor)), static_cast<int*>(at(o_long)), counters,
@@ -525,31 +673,6 @@ int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* 
     ctx.end_launch();
     TRY(ctx.launch_check("setup"));
 
-    Iterates<double> P;
-    P.m = m;
-    P.n = n;
-    P.csc_start = csc_start;
-    P.csc_row = csc_row;
-    P.csc_val = csc_val;
-    P.csr_start = csr_start;
-    P.csr_col = csr_col;
-    P.csr_val = csr_val;
-    P.c = c;
-    P.lo = lo;
-    P.hi = hi;
-    P.blo = blo;
-    P.bhi = bhi;
-    P.col_norm = col_norm;
-    P.row_norm = row_norm;
-    P.x = x;
-    P.x_bar = x_bar;
-    P.x_avg = x_avg;
-    P.dx = dx;
-    P.y = y;
-    P.y_avg = y_avg;
-    P.ax_bar = ax_bar;
-    P.partials = partials;
-    P.st = st;
     Original O{c_orig, in_obj, lo_orig, hi_orig, blo_orig, bhi_orig, col_scale, row_scale, lp->objective_offset};
     Controls ctl{o->primal_tolerance, o->dual_tolerance, o->gap_tolerance, o->restart_reduction_factor,
                  o->primal_weight_smoothing, o->restart_every, o->restart_strategy, o->adaptive_step_size,
@@ -558,70 +681,136 @@ int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* 
                 static_cast<double*>(at(o_tr[1])), static_cast<double*>(at(o_tr[2])),
                 static_cast<double*>(at(o_tr[3])), static_cast<double*>(at(o_tr[4])),
                 static_cast<int*>(at(o_tr_rs))};
-    const Plan pl = make_plan<double>(ctx, m, n, nnz, o->lanes_per_column, o->lanes_per_row,
-                                      static_cast<int*>(at(o_col_bounds)), static_cast<int*>(at(o_row_bounds)));
-    TRY(build_tiles(ctx, pl, m, n, csc_start, csr_start, static_cast<int*>(at(o_col_bounds)),
-                    static_cast<int*>(at(o_row_bounds)), chunk));
-
-    // ---- PDHG loop in restart chunks
-    const long long R = o->restart_every;
-    const long long maxit = o->max_iterations;
-    const long long full_chunks = maxit / R;
     const int poll_every = o->check_every_chunks > 0 ? o->check_every_chunks : 1;
-    long long base = 0;
-    bool done = false;
-    long long recipe[10][MC_KERNEL_KINDS] = {};
-    int inflight = 0;  // chunks launched since the last poll-able event
-    long long polled_chunks = 0;
-    int ev_idx = 0;
-    bool have_prev = false;
-    for (long long chunk = 0; chunk < full_chunks && !done; ++chunk) {
-        if (ctx.profiling) {
-            TRY(enqueue_span(ctx, P, pl, base, 0, (int)R, ctl));
-            TRY(enqueue_check(ctx, P, O, pl, R, 0, ctl, tr));
-            TRY(ctx.drain_profile());
-        } else {
-            const int key = (int)(base % 10);
-            auto it = ctx.graphs.find(key);
-            cudaGraphExec_t exec = nullptr;
-            if (it == ctx.graphs.end()) {
-                TRY(chunk_graph(ctx, P, O, pl, base, R, ctl, tr, &exec, recipe[key]));
-            } else {
-                exec = it->second;
-            }
-            CU(cudaGraphLaunch(exec, s));
-            for (int q = 0; q < MC_KERNEL_KINDS; ++q) ctx.launches[q] += recipe[key][q];
-        }
-        base += R;
-        ++inflight;
-        if (inflight >= poll_every || chunk + 1 == full_chunks) {
-            // poll the previous event (one chunk group behind), then record a new one
-            if (have_prev) {
-                CU(cudaEventSynchronize(ctx.ev_poll[ev_idx ^ 1]));
-                if (ctx.h_state[ev_idx ^ 1].done) done = true;
-            }
-            CU(cudaMemcpyAsync(&ctx.h_state[ev_idx], st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
-            CU(cudaEventRecord(ctx.ev_poll[ev_idx], s));
-            have_prev = true;
-            ev_idx ^= 1;
-            inflight = 0;
-            ++polled_chunks;
-        }
+
+    // ---- the PDHG loop
+    float* fx_avg = nullptr;
+    float* fy_avg = nullptr;
+    if (!mixed) {
+        Engine64 eng;
+        Iterates<double>& P = eng.P;
+        P.m = m;
+        P.n = n;
+        P.csc_start = csc_start;
+        P.csc_row = csc_row;
+        P.csc_val = csc_val;
+        P.csr_start = csr_start;
+        P.csr_col = csr_col;
+        P.csr_val = csr_val;
+        P.c = c;
+        P.lo = lo;
+        P.hi = hi;
+        P.blo = blo;
+        P.bhi = bhi;
+        P.col_norm = col_norm;
+        P.row_norm = row_norm;
+        P.x = x;
+        P.x_bar = x_bar;
+        P.x_avg = x_avg;
+        P.dx = dx;
+        P.y = y;
+        P.y_avg = y_avg;
+        P.ax_bar = ax_bar;
+        P.partials = partials;
+        P.st = st;
+        eng.O = O;
+        eng.pl = make_plan<double>(ctx, m, n, nnz, o->lanes_per_column, o->lanes_per_row,
+                                   static_cast<int*>(at(o_col_bounds)), static_cast<int*>(at(o_row_bounds)));
+        TRY(build_tiles(ctx, eng.pl, m, n, csc_start, csr_start, static_cast<int*>(at(o_col_bounds)),
+                        static_cast<int*>(at(o_row_bounds)), chunk));
+        TRY(run_chunks(ctx, eng, st, o->max_iterations, o->restart_every, poll_every, ctl, tr));
+    } else {
+        EngineMixed eng;
+        float* f_cscv = static_cast<float*>(at(o_f_cscv));
+        float* f_csrv = static_cast<float*>(at(o_f_csrv));
+        float* f_g = static_cast<float*>(at(o_fn[0]));
+        float* f_lo = static_cast<float*>(at(o_fn[1]));
+        float* f_hi = static_cast<float*>(at(o_fn[2]));
+        float* f_cn = static_cast<float*>(at(o_fn[3]));
+        float* f_x = static_cast<float*>(at(o_fn[4]));
+        float* f_xb = static_cast<float*>(at(o_fn[5]));
+        float* f_xa = static_cast<float*>(at(o_fn[6]));
+        float* f_dx = static_cast<float*>(at(o_fn[7]));
+        float* f_rn = static_cast<float*>(at(o_fm[0]));
+        float* f_y = static_cast<float*>(at(o_fm[1]));
+        float* f_ya = static_cast<float*>(at(o_fm[2]));
+        float* f_axb = static_cast<float*>(at(o_fm[3]));
+        float* f_rlo = static_cast<float*>(at(o_fm[4]));
+        float* f_rhi = static_cast<float*>(at(o_fm[5]));
+        float* f_yb = static_cast<float*>(at(o_fm[6]));
+        fx_avg = f_xa;
+        fy_avg = f_ya;
+        const int nbz = blocks_for(ctx, nnz + 16, kBlock) * 4;
+        ctx.begin_launch(MC_KERNEL_SETUP);
+        k_to_float<<<nbz, kBlock, 0, s>>>(nnz + 16, csc_val, f_cscv);
+        ctx.end_launch();
+        ctx.begin_launch(MC_KERNEL_SETUP);
+        k_to_float<<<nbz, kBlock, 0, s>>>(nnz + 16, csr_val, f_csrv);
+        ctx.end_launch();
+        ctx.begin_launch(MC_KERNEL_SETUP);
+        k_to_float<<<nbc, kBlock, 0, s>>>(n, col_norm, f_cn);
+        ctx.end_launch();
+        ctx.begin_launch(MC_KERNEL_SETUP);
+        k_to_float<<<nbr, kBlock, 0, s>>>(m, row_norm, f_rn);
+        ctx.end_launch();
+        for (float* z : {f_x, f_xb, f_xa, f_dx}) CU(cudaMemsetAsync(z, 0, sizeof(float) * (size_t)n, s));
+        for (float* z : {f_y, f_ya, f_axb}) CU(cudaMemsetAsync(z, 0, sizeof(float) * (size_t)m, s));
+        Iterates<float>& P = eng.P;
+        P.m = m;
+        P.n = n;
+        P.csc_start = csc_start;
+        P.csc_row = csc_row;
+        P.csc_val = f_cscv;
+        P.csr_start = csr_start;
+        P.csr_col = csr_col;
+        P.csr_val = f_csrv;
+        P.c = f_g;
+        P.lo = f_lo;
+        P.hi = f_hi;
+        P.blo = nullptr;  // the mixed dual step reads r_lo / r_hi instead
+        P.bhi = nullptr;
+        P.col_norm = f_cn;
+        P.row_norm = f_rn;
+        P.x = f_x;
+        P.x_bar = f_xb;
+        P.x_avg = f_xa;
+        P.dx = f_dx;
+        P.y = f_y;
+        P.y_avg = f_ya;
+        P.ax_bar = f_axb;
+        P.partials = partials;
+        P.st = st;
+        MixedState& M = eng.M;
+        M.x_hat = x;  // the FP64 start point becomes the first base
+        M.y_hat = y;
+        M.ax_full = ax_bar;
+        M.aty_full = dx;
+        M.c64 = c;
+        M.lo64 = lo;
+        M.hi64 = hi;
+        M.blo64 = blo;
+        M.bhi64 = bhi;
+        M.csc_val64 = csc_val;
+        M.csr_val64 = csr_val;
+        M.g = f_g;
+        M.lo = f_lo;
+        M.hi = f_hi;
+        M.r_lo = f_rlo;
+        M.r_hi = f_rhi;
+        M.yb = f_yb;
+        eng.O = O;
+        eng.pl = make_plan<float>(ctx, m, n, nnz, o->lanes_per_column, o->lanes_per_row,
+                                  static_cast<int*>(at(o_col_bounds)), static_cast<int*>(at(o_row_bounds)));
+        MC_DISPATCH_G(eng.pl.g_row, eng.nb_res_row = grid_for(ctx, k_residual_rows_mx<G>, m, kBlock / G));
+        MC_DISPATCH_G(eng.pl.g_col, eng.nb_res_col = grid_for(ctx, k_residual_cols_mx<G>, n, kBlock / G));
+        eng.nb_recenter = grid_for(ctx, k_recenter_mx, (long long)n + m, kBlock);
+        eng.nb_apply = grid_for(ctx, k_dual_apply_mx, m, kBlock);
+        // first correction LP around the start point
+        TRY(eng.residual_pass(ctx));
+        TRY(eng.recenter(ctx, 1));
+        TRY(run_chunks(ctx, eng, st, o->max_iterations, o->restart_every, poll_every, ctl, tr));
     }
-    CU(cudaStreamSynchronize(s));
     CU(cudaMemcpy(&ctx.h_state[2], st, sizeof(DevState), cudaMemcpyDeviceToHost));
-    done = ctx.h_state[2].done != 0;
-    if (!done) {
-        // the loop ran out: remaining partial chunk, then the final evaluation
-        // (pdlp.cpp:263-265); after a whole number of chunks the last check
-        // already holds the averages' residuals
-        const long long rem = maxit - full_chunks * R;
-        if (rem > 0 || full_chunks == 0) {
-            TRY(enqueue_span(ctx, P, pl, base, 0, (int)rem, ctl));
-            TRY(enqueue_check(ctx, P, O, pl, rem, 1, ctl, tr));
-            TRY(ctx.drain_profile());
-        }
-    }
     CU(cudaEventRecord(ctx.ev_c, s));
 
     // ---- outputs
@@ -629,8 +818,10 @@ int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* 
     double* xo = dev_out ? x_out : (x_out ? x_stage : nullptr);
     double* yo = dev_out ? y_out : (y_out ? y_stage : nullptr);
     if (xo || yo) {
+        const int nb = blocks_for(ctx, (long long)n + m, kBlock);
         ctx.begin_launch(MC_KERNEL_OTHER);
-        k_unscale_out<<<pl.nb_nm, kBlock, 0, s>>>(n, m, x_avg, y_avg, col_scale, row_scale, xo, yo);
+        if (mixed) k_unscale_out_mx<<<nb, kBlock, 0, s>>>(n, m, x, fx_avg, y, fy_avg, col_scale, row_scale, xo, yo);
+        else k_unscale_out<<<nb, kBlock, 0, s>>>(n, m, x_avg, y_avg, col_scale, row_scale, xo, yo);
         ctx.end_launch();
         TRY(ctx.launch_check("unscale"));
     }
@@ -679,6 +870,8 @@ int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* 
     res->restarts = S.restarts;
     res->final_primal_weight = S.omega;
     res->final_step_size = S.eta;
+    res->refinement_rounds = mixed ? S.restarts : 0;  // each restart re-centres the FP64 base
+    res->inner_iterations = mixed ? S.iter : 0;
     long long total = 0;
     for (int q = 0; q < MC_KERNEL_KINDS; ++q) {
         res->launches_by_kind[q] = ctx.launches[q];
@@ -687,7 +880,6 @@ int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* 
     }
     res->kernel_launches = total;
     res->total_ms = now_ms() - t_begin;
-    (void)polled_chunks;
     return MC_OK;
 }
 
