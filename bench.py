@@ -234,6 +234,26 @@ def run_reference_arm(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_ncu_case(args) -> None:
+    """A short profiled solve of the workload (for ncu captures of the hot
+    kernels): setup plus `--ncu-iterations` PDHG iterations."""
+    import torch
+    import mcpdlp
+    from mcpdlp import PdlpOptions, Precision
+    model = make_model(WORKLOAD["seed"])
+    ctx = mcpdlp.Context(0)
+    dm = mcpdlp.DeviceModel(model)
+    x = torch.empty(model.num_cols, dtype=torch.float64, device="cuda")
+    y = torch.empty(model.num_rows, dtype=torch.float64, device="cuda")
+    o = PdlpOptions(max_iterations=args.ncu_iterations, profile_kernels=True,
+                    precision=Precision.fp32_refine if args.precision == "fp32_refine" else Precision.fp64)
+    o.set_tolerance(TOL)
+    r = ctx.solve_device(dm, o, x, y)
+    print(json.dumps({"ncu_case": args.precision, "iterations": r.iterations,
+                      "launches": r.extra["launches_by_kind"]}), flush=True)
+    ctx.close()
+
+
 def run_engine_arm(args) -> None:
     import torch
     import mcpdlp
@@ -307,8 +327,36 @@ def run_engine_arm(args) -> None:
     h2d_bytes = (4 * (n + 1) + 12 * nnz + 8 * 3 * n + 8 * 2 * m)
     d2h_bytes = 8 * (n + m)
 
-    # ---- roofline of the dominant kernel: a profiled solve (events per launch)
-    popts = PdlpOptions(device=local, profile_kernels=True)
+    # ---- the mixed-precision form (FP32 iterations, FP64 checks), same LP
+    from mcpdlp import Precision
+    mopts = PdlpOptions(device=local, precision=Precision.fp32_refine)
+    mopts.set_tolerance(TOL)
+    if dist:
+        dist.barrier()
+    mixed_res = []
+    t0 = time.perf_counter()
+    for _ in range(max(1, args.steps)):
+        mixed_res.append(ctx.solve_device(dmodel, mopts, x, y))
+    mixed_s = max_over_ranks(dist, time.perf_counter() - t0, dev)
+    mixed_iters = sum_over_ranks(dist, float(sum(r.iterations for r in mixed_res)), dev)
+    mlast = mixed_res[-1]
+    forms = {
+        "fp64": {"time_to_tol_s": t_max / max(1, args.steps), "iterations": last.iterations,
+                 "ms_per_iteration": t_max * 1e3 / max(1, iters_all / world), "status": last.status.name,
+                 "objective_rel_err_vs_analytic": abs(last.objective - model.info["optimum"]) / abs(model.info["optimum"])},
+        "fp32_refine": {"time_to_tol_s": mixed_s / max(1, args.steps), "iterations": mlast.iterations,
+                        "ms_per_iteration": mixed_s * 1e3 / max(1, mixed_iters / world),
+                        "status": mlast.status.name, "iterations_per_s": mixed_iters / mixed_s,
+                        "objective_rel_err_vs_analytic": abs(mlast.objective - model.info["optimum"]) / abs(model.info["optimum"]),
+                        "kkt": {"primal": mlast.primal_infeasibility, "dual": mlast.dual_infeasibility,
+                                "gap": mlast.duality_gap}},
+    }
+    forms["speedup_time_to_tol_fp32_refine_vs_fp64"] = forms["fp64"]["time_to_tol_s"] / forms["fp32_refine"]["time_to_tol_s"]
+    launches += sum(r.extra["kernel_launches"] for r in mixed_res)
+
+    # ---- roofline of the dominant kernel: a profiled solve (events per launch,
+    # on the engine's stream), bounded to 2000 iterations
+    popts = PdlpOptions(device=local, profile_kernels=True, max_iterations=2000)
     popts.set_tolerance(TOL)
     prof = ctx.solve_device(dmodel, popts, x, y)
     kms = prof.extra["kernel_ms_by_kind"]
@@ -346,6 +394,7 @@ def run_engine_arm(args) -> None:
         "kkt": {"primal": last.primal_infeasibility, "dual": last.dual_infeasibility, "gap": last.duality_gap},
         "clocks": clock,
         "gpu_launches": launches,
+        "forms": forms,
         "e2e": {"value": e2e_iters / e2e_t, "unit": UNIT, "h2d_bytes_per_step": h2d_bytes,
                 "d2h_bytes_per_step": d2h_bytes, "s_per_step": e2e_t / max(1, args.steps)},
         "roofline": roofline,
@@ -364,12 +413,18 @@ def run_engine_arm(args) -> None:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ncu-case", action="store_true",
+                    help="run one short profiled solve of the workload (for ncu) and exit")
+    ap.add_argument("--ncu-iterations", type=int, default=12)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32_refine"])
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.ncu_case:
+        run_ncu_case(args)
+    elif args.impl == "reference":
         run_reference_arm(args)
     else:
         run_engine_arm(args)

@@ -212,6 +212,23 @@ int mc_pdlp_solve(const mc_lp* lp, const mc_pdlp_options* options,
                   double* primal_out, double* dual_out, mc_pdlp_result* result);
 
 /*
+ * Batched solve: `count` independent LPs of any sizes in one set of launches
+ * (no counterpart in the reference, which solves one LP per call).  The LPs
+ * are packed block-diagonally on the device and every LP runs the same
+ * algorithm as mc_pdlp_ctx_solve with its own step size, primal weight,
+ * restarts and termination.  Each lps[b] may be in host or device memory
+ * (its `memory` field); primal_out[b] / dual_out[b] (arrays of `count`
+ * pointers, entries may be NULL) receive the unscaled averages of LP b in
+ * the same memory space as lps[b].  results[b] is LP b's result.  An LP with
+ * a crossed bound (lower > upper) or a row whose activity interval over the
+ * variable box misses the row's bounds is reported
+ * MC_PDLP_INFEASIBLE_OR_UNBOUNDED at setup.  FP64 form only.
+ */
+int mc_pdlp_ctx_solve_batch(mc_pdlp_ctx* ctx, const mc_lp* lps, int32_t count,
+                            const mc_pdlp_options* options, double* const* primal_out,
+                            double* const* dual_out, mc_pdlp_result* results);
+
+/*
  * Kernel-level entry points (device pointers, the context's stream), used by
  * the parity tests and the roofline measurement.  They replace the reference's
  * file-local helpers of the same meaning.

@@ -1,0 +1,534 @@
+// Batched PDLP: many independent LPs of uneven size solved together.
+//
+// The LPs are packed block-diagonally into one CSC and one CSR (column block
+// b holds LP b's columns, row block b its rows).  Every kernel launches one
+// block per tile; a tile is a run of consecutive lines (columns or rows) of
+// ONE LP, so a block reads that LP's scalars once (its DevState: eta, omega,
+// averaging count, restart and termination state) and writes its reduction
+// partial to its own slot.  The per-LP reductions then read the LP's tile
+// range in order: every LP follows the reference algorithm
+// (src/lp/first_order/pdlp.cpp:139-276) on its own -- own step size, own
+// primal weight, own restarts and termination -- exactly as if it were solved
+// alone, and the results are run-to-run deterministic.  All LPs advance in
+// lockstep; an LP that has terminated costs one flag read per tile.
+//
+// The row and column work inside a tile is the single-LP kernels' (lanes per
+// line, cache policies, fused updates), so the per-nonzero cost is the same.
+#pragma once
+
+#include "common.cuh"
+#include "iter_kernels.cuh"
+#include "setup_kernels.cuh"
+
+namespace mc {
+
+struct TileTable {
+    const int* lp;     // [ntiles] owning LP
+    const int* l0;     // [ntiles] first line
+    const int* l1;     // [ntiles] one past the last line
+    const int* first;  // [nlp + 1] tile range of each LP
+    int ntiles;
+};
+
+struct BatchRefs {
+    DevState* st;              // [nlp]
+    const double* offset;      // [nlp] objective offsets
+    int* flags;                // [nlp] setup certificates: 1 crossed bounds, 2 row activity
+    TileTable cols, rows;
+    int nlp;
+};
+
+constexpr int kMaxTiles = 1 << 17;  // per-slot capacity of the batch partials buffer
+
+// Lines of this block's tile, G lanes per line; every thread of the block
+// makes the same number of trips (the shuffles need all lanes).
+#define MC_TILE_LINES(TT, LINE, VALID, SUB)                                                          \
+    const int SUB = threadIdx.x % G;                                                                \
+    const int tl1_ = TT.l1[blockIdx.x];                                                             \
+    for (int base_ = TT.l0[blockIdx.x], LINE = 0;                                                   \
+         base_ < tl1_ && ((LINE = base_ + (int)(threadIdx.x / G)), true); base_ += kBlock / G)     \
+        if (const bool VALID = LINE < tl1_; true)
+
+// ------------------------------------------------------------------ primal
+template <int G, bool STEP>
+__global__ void __launch_bounds__(kBlock) kb_primal(Iterates<double> P, BatchRefs B, int k) {
+    __shared__ double scratch[32];
+    const int lp = B.cols.lp[blockIdx.x];
+    const DevState* st = B.st + lp;
+    if (st->done) {
+        if (STEP && threadIdx.x == 0) P.partials[SLOT_DX * kMaxTiles + blockIdx.x] = 0.0;
+        return;
+    }
+    const double step = st->eta / st->omega;
+    const double cnt = (double)(st->avg_count + k + 1);
+    const unsigned long long pol = policy_keep();
+    double acc = 0.0;
+    MC_TILE_LINES(B.cols, j, valid, sub) {
+        const bool owner = valid && sub == 0;
+        double cn = 1.0, cj = 0.0, xo = 0.0, lj = 0.0, hj = 0.0, xa = 0.0;
+        if (owner) {
+            cn = ld_stream(P.col_norm + j);
+            cj = ld_stream(P.c + j);
+            xo = ld_stream(P.x + j);
+            lj = ld_stream(P.lo + j);
+            hj = ld_stream(P.hi + j);
+            xa = ld_stream(P.x_avg + j);
+        }
+        const double aty = line_dot<G>(P.csc_start, P.csc_row, P.csc_val, P.y, j, valid, sub, pol);
+        if (owner) {
+            const double g = __dadd_rn(cj, aty);
+            const double tau = __ddiv_rn(step, cn);
+            const double xp = clampv(__dsub_rn(xo, __dmul_rn(tau, g)), lj, hj);
+            const double d = __dsub_rn(xp, xo);
+            if (STEP) {
+                st_keep(P.dx + j, d, pol);
+                acc += __dmul_rn(__dmul_rn(cn, d), d);
+            }
+            st_stream(P.x + j, xp);
+            st_keep(P.x_bar + j, __dsub_rn(__dmul_rn(2.0, xp), xo), pol);
+            st_stream(P.x_avg + j, __dadd_rn(xa, __ddiv_rn(__dsub_rn(xp, xa), cnt)));
+        }
+    }
+    if (STEP) {
+        acc = block_reduce(acc, scratch, OpSum());
+        if (threadIdx.x == 0) P.partials[SLOT_DX * kMaxTiles + blockIdx.x] = acc;
+    }
+}
+
+// -------------------------------------------------------------------- dual
+template <int G>
+__global__ void __launch_bounds__(kBlock) kb_dual(Iterates<double> P, BatchRefs B, int k) {
+    const int lp = B.rows.lp[blockIdx.x];
+    const DevState* st = B.st + lp;
+    if (st->done) return;
+    const double sg = st->eta * st->omega;
+    const double cnt = (double)(st->avg_count + k + 1);
+    const unsigned long long pol = policy_keep();
+    MC_TILE_LINES(B.rows, i, valid, sub) {
+        RowData<double> r{};
+        if (valid && sub == 0) r = load_row(P, i);
+        const double ax = line_dot<G>(P.csr_start, P.csr_col, P.csr_val, P.x_bar, i, valid, sub, pol);
+        if (valid && sub == 0) dual_update(P, i, r, ax, sg, cnt, pol);
+    }
+}
+
+template <int G>
+__global__ void __launch_bounds__(kBlock) kb_dual_probe(Iterates<double> P, BatchRefs B) {
+    __shared__ double scratch[32];
+    const int lp = B.rows.lp[blockIdx.x];
+    if (B.st[lp].done) {
+        if (threadIdx.x == 0) P.partials[SLOT_ADX * kMaxTiles + blockIdx.x] = 0.0;
+        return;
+    }
+    const unsigned long long pol = policy_keep();
+    double acc = 0.0;
+    MC_TILE_LINES(B.rows, i, valid, sub) {
+        double axb, adx;
+        line_dot2<G>(P.csr_start, P.csr_col, P.csr_val, P.x_bar, P.dx, i, valid, sub, axb, adx, pol);
+        if (valid && sub == 0) {
+            P.ax_bar[i] = axb;
+            acc += __ddiv_rn(__dmul_rn(adx, adx), P.row_norm[i]);
+        }
+    }
+    acc = block_reduce(acc, scratch, OpSum());
+    if (threadIdx.x == 0) P.partials[SLOT_ADX * kMaxTiles + blockIdx.x] = acc;
+}
+
+// one block per LP: the adaptive eta rule (pdlp.cpp:207-219) on the LP's sums
+__global__ void kb_step_size(const double* __restrict__ partials, BatchRefs B, Controls ctl) {
+    __shared__ double scratch[32];
+    const int lp = blockIdx.x;
+    DevState* st = B.st + lp;
+    if (st->done) return;
+    const int c0 = B.cols.first[lp], c1 = B.cols.first[lp + 1];
+    const int r0 = B.rows.first[lp], r1 = B.rows.first[lp + 1];
+    const double dxn = reduce_partials(partials + SLOT_DX * kMaxTiles + c0, c1 - c0, scratch, OpSum());
+    const double adx = reduce_partials(partials + SLOT_ADX * kMaxTiles + r0, r1 - r0, scratch, OpSum());
+    if (threadIdx.x == 0 && ctl.adaptive_step && dxn > 1e-14 && adx > 1e-14) {
+        const double L = sqrt(adx / dxn);
+        if (L > 1e-6) {
+            const double target = 0.95 / L;
+            const double eta = st->eta;
+            if (target < eta) st->eta = maxv(0.1, maxv(target, eta * 0.8));
+            else if (target > 1.05 * eta && eta < 0.99) st->eta = minv(0.99, eta * 1.05);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) kb_dual_apply(Iterates<double> P, BatchRefs B, int k) {
+    const int lp = B.rows.lp[blockIdx.x];
+    const DevState* st = B.st + lp;
+    if (st->done) return;
+    const double sg = st->eta * st->omega;
+    const double cnt = (double)(st->avg_count + k + 1);
+    const unsigned long long pol = policy_keep();
+    for (int i = B.rows.l0[blockIdx.x] + threadIdx.x; i < B.rows.l1[blockIdx.x]; i += blockDim.x)
+        dual_update(P, i, P.ax_bar[i], sg, cnt, pol);
+}
+
+// --------------------------------------------------------------- residuals
+template <int G>
+__global__ void __launch_bounds__(kBlock) kb_residual_rows(Iterates<double> P, Original O, BatchRefs B) {
+    __shared__ double scratch[32];
+    const int lp = B.rows.lp[blockIdx.x];
+    RowTerms acc;
+    if (!B.st[lp].done) {
+        MC_TILE_LINES(B.rows, i, valid, sub) {
+            double s = 0.0;
+            if (valid) {
+                const int b = P.csr_start[i], e = P.csr_start[i + 1];
+                for (int p = b + sub; p < e; p += G) s = fma(P.csr_val[p], P.x_avg[P.csr_col[p]], s);
+            }
+            s = group_sum<G>(s);
+            if (valid && sub == 0) acc.add(O, i, s, P.y_avg[i]);
+        }
+    }
+    acc.vmax = block_reduce(acc.vmax, scratch, OpMax());
+    acc.dsum = block_reduce(acc.dsum, scratch, OpSum());
+    acc.bad = block_reduce(acc.bad, scratch, OpSum());
+    if (threadIdx.x == 0) {
+        P.partials[SLOT_ROW_MAX * kMaxTiles + blockIdx.x] = acc.vmax;
+        P.partials[SLOT_ROW_DOBJ * kMaxTiles + blockIdx.x] = acc.dsum;
+        P.partials[SLOT_NAN * kMaxTiles + blockIdx.x] = acc.bad;
+    }
+}
+
+template <int G>
+__global__ void __launch_bounds__(kBlock) kb_residual_cols(Iterates<double> P, Original O, BatchRefs B) {
+    __shared__ double scratch[32];
+    const int lp = B.cols.lp[blockIdx.x];
+    ColTerms acc;
+    if (!B.st[lp].done) {
+        MC_TILE_LINES(B.cols, j, valid, sub) {
+            double s = 0.0;
+            if (valid) {
+                const int b = P.csc_start[j], e = P.csc_start[j + 1];
+                for (int p = b + sub; p < e; p += G) s = fma(P.csc_val[p], P.y_avg[P.csc_row[p]], s);
+            }
+            s = group_sum<G>(s);
+            if (valid && sub == 0) acc.add(O, j, s, P.x_avg[j]);
+        }
+    }
+    acc.vmax = block_reduce(acc.vmax, scratch, OpMax());
+    acc.dres = block_reduce(acc.dres, scratch, OpSum());
+    acc.pobj = block_reduce(acc.pobj, scratch, OpSum());
+    acc.dobj = block_reduce(acc.dobj, scratch, OpSum());
+    acc.bad = block_reduce(acc.bad, scratch, OpSum());
+    if (threadIdx.x == 0) {
+        P.partials[SLOT_COL_MAX * kMaxTiles + blockIdx.x] = acc.vmax;
+        P.partials[SLOT_COL_DRES * kMaxTiles + blockIdx.x] = acc.dres;
+        P.partials[SLOT_COL_POBJ * kMaxTiles + blockIdx.x] = acc.pobj;
+        P.partials[SLOT_COL_DOBJ * kMaxTiles + blockIdx.x] = acc.dobj;
+        P.partials[SLOT_B * kMaxTiles + blockIdx.x] = acc.bad;
+    }
+}
+
+// One block per LP: KKT scalars, termination, restart and primal weight of
+// that LP (pdlp.cpp:229-261), as k_finalize for a single LP.
+__global__ void kb_finalize(const double* __restrict__ partials, BatchRefs B, long long span, int final_pass,
+                            Controls ctl) {
+    __shared__ double scratch[32];
+    const int lp = blockIdx.x;
+    DevState* st = B.st + lp;
+    if (st->done) return;
+    const int c0 = B.cols.first[lp], nc = B.cols.first[lp + 1] - c0;
+    const int r0 = B.rows.first[lp], nr = B.rows.first[lp + 1] - r0;
+    const double row_max = reduce_partials(partials + SLOT_ROW_MAX * kMaxTiles + r0, nr, scratch, OpMax());
+    const double row_dobj = reduce_partials(partials + SLOT_ROW_DOBJ * kMaxTiles + r0, nr, scratch, OpSum());
+    const double bad_r = reduce_partials(partials + SLOT_NAN * kMaxTiles + r0, nr, scratch, OpSum());
+    const double col_max = reduce_partials(partials + SLOT_COL_MAX * kMaxTiles + c0, nc, scratch, OpMax());
+    const double col_dres = reduce_partials(partials + SLOT_COL_DRES * kMaxTiles + c0, nc, scratch, OpSum());
+    const double col_pobj = reduce_partials(partials + SLOT_COL_POBJ * kMaxTiles + c0, nc, scratch, OpSum());
+    const double col_dobj = reduce_partials(partials + SLOT_COL_DOBJ * kMaxTiles + c0, nc, scratch, OpSum());
+    const double bad_c = reduce_partials(partials + SLOT_B * kMaxTiles + c0, nc, scratch, OpSum());
+    if (threadIdx.x != 0) return;
+    const double offset = B.offset[lp];
+    const double primal = maxv(row_max, col_max);
+    const double dual = sqrt(col_dres) / st->c_scale;
+    const double pobj = offset + col_pobj;
+    const double dobj = (offset + row_dobj) + col_dobj;
+    const double gap = fabs(pobj - dobj) / (1.0 + fabs(pobj) + fabs(dobj));
+    const double score = maxv(maxv(primal, dual), gap);
+    st->primal_infeas = primal;
+    st->dual_infeas = dual;
+    st->gap = gap;
+    st->objective = pobj;
+    st->dual_objective = dobj;
+    st->score = score;
+    st->restart_pending = 0;
+    const long long isr = st->iters_since_restart + span;
+    if (bad_r + bad_c > 0.0 || !isfinite(score)) {
+        st->nonfinite = 1;
+        st->done = 1;
+        st->status = 3;
+    } else if (!final_pass && primal <= ctl.primal_tol && dual <= ctl.dual_tol && gap <= ctl.gap_tol) {
+        st->done = 1;
+        st->status = 0;
+    } else if (!final_pass) {
+        const bool do_restart =
+            ctl.strategy == 2 ||
+            (ctl.strategy == 1 && (score <= ctl.restart_reduction * st->last_restart_score ||
+                                   (isr >= 5 * ctl.restart_every && score < st->last_restart_score)));
+        if (do_restart) {
+            if (ctl.adaptive_weight && primal > 1e-12 && dual > 1e-12) {
+                const double ratio = clampv(sqrt(primal / dual), 0.05, 20.0);
+                st->omega = clampv(st->omega * pow(ratio, ctl.weight_smoothing), 1e-6, 1e6);
+            }
+            st->restart_pending = 1;
+            st->avg_count = 0;
+            st->iters_since_restart = 0;
+            st->last_restart_score = score;
+            st->restarts += 1;
+        } else {
+            st->avg_count += span;
+            st->iters_since_restart = isr;
+        }
+    }
+    st->iter += span;
+    if (!final_pass) st->checks += 1;
+}
+
+// restart to the average, per tile (columns tiles then row tiles)
+__global__ void __launch_bounds__(kBlock) kb_restart_copy(Iterates<double> P, BatchRefs B) {
+    const bool col = blockIdx.x < (unsigned)B.cols.ntiles;
+    const int t = col ? blockIdx.x : blockIdx.x - B.cols.ntiles;
+    const TileTable& T = col ? B.cols : B.rows;
+    const DevState* st = B.st + T.lp[t];
+    if (!st->restart_pending || st->done) return;
+    for (int l = T.l0[t] + threadIdx.x; l < T.l1[t]; l += blockDim.x) {
+        if (col) P.x[l] = P.x_avg[l];
+        else P.y[l] = P.y_avg[l];
+    }
+}
+
+// ------------------------------------------------------------------ setup
+// Ruiz per LP: line maxima of a tile, per-LP check, deltas and rescale skip
+// LPs whose Ruiz has converged (ruiz_scaling.cpp:167-218 per LP).
+__global__ void kb_ruiz_line_max(const int* __restrict__ start, const double* __restrict__ value,
+                                 double* __restrict__ norm, double* __restrict__ partials, int slot,
+                                 TileTable T, const DevState* __restrict__ st) {
+    __shared__ double scratch[32];
+    double err = 0.0;
+    if (!st[T.lp[blockIdx.x]].ruiz_done) {
+        for (int j = T.l0[blockIdx.x] + threadIdx.x; j < T.l1[blockIdx.x]; j += blockDim.x) {
+            double mx = 0.0;
+            for (int p = start[j]; p < start[j + 1]; ++p) mx = maxv(mx, fabs(value[p]));
+            if (mx == 0.0) mx = 1.0;
+            norm[j] = mx;
+            err = maxv(err, fabs(1.0 - mx));
+        }
+    }
+    err = block_reduce(err, scratch, OpMax());
+    if (threadIdx.x == 0) partials[slot * kMaxTiles + blockIdx.x] = err;
+}
+
+__global__ void kb_ruiz_check(const double* __restrict__ partials, BatchRefs B, double tolerance) {
+    __shared__ double scratch[32];
+    const int lp = blockIdx.x;
+    DevState* st = B.st + lp;
+    if (st->ruiz_done) return;
+    const int c0 = B.cols.first[lp], nc = B.cols.first[lp + 1] - c0;
+    const int r0 = B.rows.first[lp], nr = B.rows.first[lp + 1] - r0;
+    const double c = reduce_partials(partials + SLOT_A * kMaxTiles + c0, nc, scratch, OpMax());
+    const double r = reduce_partials(partials + SLOT_B * kMaxTiles + r0, nr, scratch, OpMax());
+    if (threadIdx.x == 0) {
+        if (r < tolerance && c < tolerance) st->ruiz_done = 1;
+        else st->ruiz_passes += 1;
+    }
+}
+
+__global__ void kb_ruiz_deltas(double* __restrict__ norm, double* __restrict__ scale, TileTable T,
+                               const DevState* __restrict__ st) {
+    if (st[T.lp[blockIdx.x]].ruiz_done) return;
+    for (int j = T.l0[blockIdx.x] + threadIdx.x; j < T.l1[blockIdx.x]; j += blockDim.x) {
+        const double d = 1.0 / sqrt(norm[j]);
+        norm[j] = d;
+        scale[j] *= d;
+    }
+}
+
+__global__ void kb_ruiz_rescale(const int* __restrict__ start, const int* __restrict__ inner,
+                                double* __restrict__ value, const double* __restrict__ delta_outer,
+                                const double* __restrict__ delta_inner, TileTable T,
+                                const DevState* __restrict__ st) {
+    if (st[T.lp[blockIdx.x]].ruiz_done) return;
+    for (int j = T.l0[blockIdx.x] + threadIdx.x; j < T.l1[blockIdx.x]; j += blockDim.x) {
+        const double dout = delta_outer[j];
+        for (int p = start[j]; p < start[j + 1]; ++p)
+            value[p] = __dmul_rn(value[p], __dmul_rn(delta_inner[inner[p]], dout));
+    }
+}
+
+// Column setup of a tile (k_setup_cols per LP) plus the crossed-bound
+// certificate: a column with lower > upper makes its LP infeasible.
+__global__ void kb_setup_cols(const int* __restrict__ col_start, const double* __restrict__ value,
+                              const double* __restrict__ obj_in, const double* __restrict__ lo_in,
+                              const double* __restrict__ hi_in, const double* __restrict__ col_scale,
+                              const double* __restrict__ obj_sign, Iterates<double> P, Original O,
+                              double* __restrict__ partials, BatchRefs B) {
+    __shared__ double scratch[32];
+    const int lp = B.cols.lp[blockIdx.x];
+    const double sign = obj_sign[lp];
+    double cmax = 0.0, comax = 0.0;
+    int crossed = 0;
+    for (int j = B.cols.l0[blockIdx.x] + threadIdx.x; j < B.cols.l1[blockIdx.x]; j += blockDim.x) {
+        const double s = col_scale[j];
+        const double inv = 1.0 / s;
+        const double l0 = lo_in[j], h0 = hi_in[j];
+        const double ls = isfinite(l0) ? __dmul_rn(l0, inv) : l0;
+        const double hs = isfinite(h0) ? __dmul_rn(h0, inv) : h0;
+        const double lsent = isinf(ls) ? -kBig : ls;
+        const double hsent = isinf(hs) ? kBig : hs;
+        const_cast<double*>(P.lo)[j] = lsent;
+        const_cast<double*>(P.hi)[j] = hsent;
+        const_cast<double*>(O.lo)[j] = isinf(l0) ? -kBig : l0;
+        const_cast<double*>(O.hi)[j] = isinf(h0) ? kBig : h0;
+        if (l0 > h0) crossed = 1;
+        const double cj = sign * __dmul_rn(obj_in[j], s);
+        const_cast<double*>(P.c)[j] = cj;
+        cmax = maxv(cmax, fabs(cj));
+        const double co = sign * obj_in[j];
+        const_cast<double*>(O.c)[j] = co;
+        comax = maxv(comax, fabs(co));
+        double nrm = 0.0;
+        for (int p = col_start[j]; p < col_start[j + 1]; ++p) nrm += fabs(value[p]);
+        const_cast<double*>(P.col_norm)[j] = (nrm < 1e-12) ? 1.0 : nrm;
+        const double x0 = clampv(0.0, lsent, hsent);
+        P.x[j] = x0;
+        P.x_avg[j] = x0;
+    }
+    if (crossed) atomicOr(B.flags + lp, 1);
+    cmax = block_reduce(cmax, scratch, OpMax());
+    if (threadIdx.x == 0) partials[SLOT_A * kMaxTiles + blockIdx.x] = cmax;
+    comax = block_reduce(comax, scratch, OpMax());
+    if (threadIdx.x == 0) partials[SLOT_B * kMaxTiles + blockIdx.x] = comax;
+}
+
+// Row setup of a tile (k_setup_rows per LP) plus the row-activity
+// certificate: with every variable in its (original) box a row's activity
+// lies in [sum min(a l, a u), sum max(a l, a u)]; if that interval misses the
+// row's [b_lo, b_hi] (beyond a relative 1e-9) the LP is infeasible.
+__global__ void kb_setup_rows(const int* __restrict__ row_start, const int* __restrict__ col_index,
+                              const double* __restrict__ value, const double* __restrict__ rlo_in,
+                              const double* __restrict__ rhi_in, const double* __restrict__ row_scale,
+                              const double* __restrict__ col_scale, const double* __restrict__ lo_in,
+                              const double* __restrict__ hi_in, Iterates<double> P, Original O,
+                              double* __restrict__ partials, BatchRefs B) {
+    __shared__ double scratch[32];
+    const int lp = B.rows.lp[blockIdx.x];
+    double bmax = 0.0;
+    int infeasible = 0;
+    for (int i = B.rows.l0[blockIdx.x] + threadIdx.x; i < B.rows.l1[blockIdx.x]; i += blockDim.x) {
+        const double s = row_scale[i];
+        const double l0 = rlo_in[i], h0 = rhi_in[i];
+        const double ls = isfinite(l0) ? __dmul_rn(l0, s) : l0;
+        const double hs = isfinite(h0) ? __dmul_rn(h0, s) : h0;
+        const double lsent = isinf(ls) ? -kBig : ls;
+        const double hsent = isinf(hs) ? kBig : hs;
+        const_cast<double*>(P.blo)[i] = lsent;
+        const_cast<double*>(P.bhi)[i] = hsent;
+        const_cast<double*>(O.blo)[i] = isinf(l0) ? -kBig : l0;
+        const_cast<double*>(O.bhi)[i] = isinf(h0) ? kBig : h0;
+        if (fabs(lsent) < 1e299) bmax = maxv(bmax, fabs(lsent));
+        if (fabs(hsent) < 1e299) bmax = maxv(bmax, fabs(hsent));
+        double nrm = 0.0, amin = 0.0, amax = 0.0, mag = 0.0;
+        for (int p = row_start[i]; p < row_start[i + 1]; ++p) {
+            nrm += fabs(value[p]);
+            // original coefficient and bounds: a = value / (row_scale * col_scale)
+            const int j = col_index[p];
+            const double a = value[p] / (s * col_scale[j]);
+            const double lj = lo_in[j], hj = hi_in[j];
+            const double t1 = a * lj, t2 = a * hj;  // +-inf when unbounded
+            amin += (a > 0) ? t1 : t2;
+            amax += (a > 0) ? t2 : t1;
+            mag += fabs(a) * maxv(isfinite(lj) ? fabs(lj) : 0.0, isfinite(hj) ? fabs(hj) : 0.0);
+        }
+        const_cast<double*>(P.row_norm)[i] = (nrm < 1e-12) ? 1.0 : nrm;
+        const double slack = 1e-9 * (1.0 + mag + maxv(isfinite(l0) ? fabs(l0) : 0.0, isfinite(h0) ? fabs(h0) : 0.0));
+        if ((isfinite(l0) && amax < l0 - slack) || (isfinite(h0) && amin > h0 + slack)) infeasible = 1;
+        P.y[i] = 0.0;
+        P.y_avg[i] = 0.0;
+    }
+    if (infeasible) atomicOr(B.flags + lp, 2);
+    bmax = block_reduce(bmax, scratch, OpMax());
+    if (threadIdx.x == 0) partials[SLOT_C * kMaxTiles + blockIdx.x] = bmax;
+}
+
+// per-LP scalars (k_setup_scalars per LP); an LP with a certificate is
+// terminated at once as infeasible_or_unbounded
+__global__ void kb_setup_scalars(const double* __restrict__ partials, BatchRefs B, double initial_primal_weight,
+                                 double step_size_reduction) {
+    __shared__ double scratch[32];
+    const int lp = blockIdx.x;
+    DevState* st = B.st + lp;
+    const int c0 = B.cols.first[lp], nc = B.cols.first[lp + 1] - c0;
+    const int r0 = B.rows.first[lp], nr = B.rows.first[lp + 1] - r0;
+    const double cmax = reduce_partials(partials + SLOT_A * kMaxTiles + c0, nc, scratch, OpMax());
+    const double comax = reduce_partials(partials + SLOT_B * kMaxTiles + c0, nc, scratch, OpMax());
+    const double bmax = reduce_partials(partials + SLOT_C * kMaxTiles + r0, nr, scratch, OpMax());
+    if (threadIdx.x == 0) {
+        const double c_norm = maxv(1.0, cmax);
+        const double b_norm = maxv(1.0, bmax);
+        st->c_norm_inf = c_norm;
+        st->b_norm_inf = b_norm;
+        st->c_scale = maxv(1.0, comax);
+        st->omega = (initial_primal_weight > 0.0) ? initial_primal_weight
+                                                  : clampv(sqrt(c_norm / b_norm), 0.01, 100.0);
+        st->eta = clampv(step_size_reduction, 0.1, 0.99);
+        st->last_restart_score = 1e300;
+        st->primal_infeas = st->dual_infeas = st->gap = 1e300;
+        st->iter = 0;
+        st->avg_count = 0;
+        st->iters_since_restart = 0;
+        st->restarts = 0;
+        st->checks = 0;
+        st->restart_pending = 0;
+        st->nonfinite = 0;
+        if (B.flags[lp]) {
+            st->done = 1;
+            st->status = 2;  // infeasible_or_unbounded, certified at setup
+        } else {
+            st->done = 0;
+            st->status = 1;
+        }
+    }
+}
+
+// per-tile unscaled output (k_unscale_out over the tile's lines)
+__global__ void kb_unscale_out(Iterates<double> P, const double* __restrict__ col_scale,
+                               const double* __restrict__ row_scale, double* __restrict__ x_out,
+                               double* __restrict__ y_out, BatchRefs B) {
+    const bool col = blockIdx.x < (unsigned)B.cols.ntiles;
+    const int t = col ? blockIdx.x : blockIdx.x - B.cols.ntiles;
+    const TileTable& T = col ? B.cols : B.rows;
+    for (int l = T.l0[t] + threadIdx.x; l < T.l1[t]; l += blockDim.x) {
+        if (col) x_out[l] = __dmul_rn(P.x_avg[l], col_scale[l]);
+        else y_out[l] = __dmul_rn(P.y_avg[l], row_scale[l]);
+    }
+}
+
+// shift a packed LP's CSC indices into the packed numbering
+__global__ void kb_shift_indices(int* __restrict__ col_start, int* __restrict__ row_index, int ncols, long long nnz,
+                                 int nnz_offset, int row_offset) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nnz + ncols;
+         t += (long long)gridDim.x * blockDim.x) {
+        if (t < nnz) row_index[t] += row_offset;
+        else col_start[t - nnz] += nnz_offset;
+    }
+}
+
+// the packed loop's poll flag: done once every LP is done
+__global__ void kb_all_done(const DevState* __restrict__ st, int nlp, DevState* __restrict__ global) {
+    __shared__ int running;
+    if (threadIdx.x == 0) running = 0;
+    __syncthreads();
+    int c = 0;
+    for (int b = threadIdx.x; b < nlp; b += blockDim.x) c += st[b].done ? 0 : 1;
+    if (c) atomicAdd(&running, c);
+    __syncthreads();
+    if (threadIdx.x == 0) global->done = running == 0 ? 1 : 0;
+}
+
+#undef MC_TILE_LINES
+
+}  // namespace mc

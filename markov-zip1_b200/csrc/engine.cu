@@ -182,6 +182,7 @@ int pick_lanes(double mean_len) {
 }  // namespace mc
 
 #include "solve.cuh"
+#include "batch.cuh"
 #include "kernel_api.cuh"
 
 using namespace mc;
@@ -273,6 +274,14 @@ int mc_pdlp_ctx_solve(mc_pdlp_ctx* c, const mc_lp* lp, const mc_pdlp_options* op
     DeviceGuard guard(ctx->device);
     return solve_lp(*ctx, lp, options, initial_primal, initial_dual, primal_out, dual_out, result,
                     trace);
+}
+
+int mc_pdlp_ctx_solve_batch(mc_pdlp_ctx* c, const mc_lp* lps, int32_t count, const mc_pdlp_options* options,
+                            double* const* primal_out, double* const* dual_out, mc_pdlp_result* results) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(c);
+    if (!ctx) return set_error(MC_ERR_INVALID_ARGUMENT, "context is NULL");
+    DeviceGuard guard(ctx->device);
+    return solve_batch(*ctx, lps, count, options, primal_out, dual_out, results);
 }
 
 int mc_pdlp_solve(const mc_lp* lp, const mc_pdlp_options* options, const double* initial_primal,

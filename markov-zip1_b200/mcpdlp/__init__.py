@@ -229,6 +229,24 @@ class Context:
             x, y = np.zeros(0), np.zeros(0)
         return _result_from(res, x, y, trace)
 
+    def solve_batch(self, models: list, options: Optional[PdlpOptions] = None) -> list:
+        """Solve many independent LPs together (mc_pdlp_ctx_solve_batch): one
+        PdlpResult per model, each from its own run of the algorithm."""
+        options = options or PdlpOptions()
+        o = options.to_struct()
+        count = len(models)
+        lps = (_abi.McLp * count)()
+        xs = [np.zeros(mm.num_cols) for mm in models]
+        ys = [np.zeros(mm.num_rows) for mm in models]
+        for b, mm in enumerate(models):
+            lps[b] = mm.to_struct()
+        xp = (C.c_void_p * count)(*[a.ctypes.data if len(a) else None for a in xs])
+        yp = (C.c_void_p * count)(*[a.ctypes.data if len(a) else None for a in ys])
+        res = (_abi.McPdlpResult * count)()
+        _raise(self._lib.mc_pdlp_ctx_solve_batch(self._h, C.addressof(lps), count, C.addressof(o),
+                                                 C.addressof(xp), C.addressof(yp), C.addressof(res)))
+        return [_result_from(res[b], xs[b], ys[b]) for b in range(count)]
+
     def solve_device(self, dlp: "DeviceModel", options: Optional[PdlpOptions] = None,
                      primal_out=None, dual_out=None) -> PdlpResult:
         """solve_pdlp on a device-resident model (torch CUDA tensors); the

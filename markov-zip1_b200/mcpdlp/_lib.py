@@ -52,6 +52,7 @@ ENGINE_SIGNATURES = {
     "mc_pdlp_ctx_destroy": ([_VP], C.c_int),
     "mc_pdlp_ctx_solve": ([_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP], C.c_int),
     "mc_pdlp_solve": ([_VP, _VP, _VP, _VP, _VP, _VP, _VP], C.c_int),
+    "mc_pdlp_ctx_solve_batch": ([_VP, _VP, C.c_int32, _VP, _VP, _VP, _VP], C.c_int),
     "mc_spmv_csr": ([_VP, _I32, _I32, _VP, _VP, _VP, _VP, _VP], C.c_int),
     "mc_csc_to_csr": ([_VP, _I32, _I32, _I64, _VP, _VP, _VP, _VP, _VP, _VP], C.c_int),
     "mc_ruiz_equilibrate": ([_VP, _I32, _I32, _I64, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP,

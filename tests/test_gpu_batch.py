@@ -1,0 +1,91 @@
+"""Batched solves (mc_pdlp_ctx_solve_batch) vs the oracle (needs a B200).
+
+Every LP of a batch runs the reference algorithm on its own, so each result
+must match the oracle's solve of that LP alone: same status and objective
+within 1e-6 relative at 1e-8 KKT.  Node variants with a crossed bound are
+infeasible; the reference runs them to its iteration limit, the batch
+certifies them at setup (status infeasible_or_unbounded).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import mcpdlp
+from conftest import options, rel
+from mcpdlp import PdlpOptions, PdlpStatus, generators
+from test_oracle import synthetic
+
+pytestmark = pytest.mark.gpu
+
+
+def opts(tol: float, **kw) -> PdlpOptions:
+    o = PdlpOptions(**kw)
+    o.set_tolerance(tol)
+    return o
+
+
+def test_uneven_batch_matches_solo_solves(gpu_ctx, oracle):
+    models = generators.batch_part1(5, count=10, m_range=(100, 600))
+    res = gpu_ctx.solve_batch(models, opts(1e-8))
+    assert len(res) == len(models)
+    for m, r in zip(models, res):
+        cpu = oracle.solve(m, options(1e-8))
+        assert r.status == cpu.status == PdlpStatus.optimal, m.name
+        assert rel(r.objective, cpu.objective) <= 1e-6, m.name
+        assert rel(r.objective, m.info["optimum"]) <= 1e-6, m.name
+        assert max(r.primal_infeasibility, r.dual_infeasibility, r.duality_gap) <= 1e-8
+        assert len(r.primal) == m.num_cols and len(r.dual) == m.num_rows
+
+
+def test_node_variants_status_and_objective(gpu_ctx, oracle):
+    base, variants, _ = generators.batch_part2(2, variants=20, m=400, n=1200, k=8)
+    res = gpu_ctx.solve_batch(variants, opts(1e-6))
+    for v, r in zip(variants, res):
+        crossed = bool(np.any(v.var_lower > v.var_upper))
+        if crossed:
+            assert r.status == PdlpStatus.infeasible_or_unbounded, v.name
+            continue
+        cpu = oracle.solve(v, options(1e-6, max_iterations=20000))
+        assert r.status == cpu.status, v.name
+        if cpu.status == PdlpStatus.optimal:
+            assert rel(r.objective, cpu.objective) <= 1e-4, v.name
+
+
+def test_row_activity_certificate(gpu_ctx):
+    """x1 + x2 = 5 with 0 <= x <= 2: the row's activity interval [0, 4] misses 5."""
+    bad = mcpdlp.from_triplets(1, 2, [0, 0], [0, 1], [1.0, 1.0], objective=[1.0, 1.0],
+                               var_lower=[0.0, 0.0], var_upper=[2.0, 2.0], row_lower=[5.0],
+                               row_upper=[5.0])
+    good = synthetic("small_s7")
+    res = gpu_ctx.solve_batch([bad, good], opts(1e-6))
+    assert res[0].status == PdlpStatus.infeasible_or_unbounded
+    assert res[1].status == PdlpStatus.optimal
+
+
+def test_batch_of_one_agrees_with_single_solve(gpu_ctx):
+    m = synthetic("config0_s1")
+    single = gpu_ctx.solve(m, opts(1e-8))
+    (b,) = gpu_ctx.solve_batch([m], opts(1e-8))
+    assert b.status == single.status == PdlpStatus.optimal
+    assert rel(b.objective, single.objective) <= 1e-7
+
+
+def test_batch_deterministic(gpu_ctx):
+    models = generators.batch_part1(6, count=6, m_range=(100, 400))
+    a = gpu_ctx.solve_batch(models, opts(1e-8))
+    b = gpu_ctx.solve_batch(models, opts(1e-8))
+    for x, y in zip(a, b):
+        assert x.iterations == y.iterations and x.objective == y.objective
+        assert np.array_equal(x.primal, y.primal)
+
+
+def test_batch_iteration_limit_and_trivial_members(gpu_ctx):
+    empty = mcpdlp.Model(0, 2, np.zeros(3, np.int32), np.zeros(0, np.int32), np.zeros(0),
+                         np.ones(2), np.zeros(2), np.ones(2), np.zeros(0), np.zeros(0))
+    m = synthetic("small_s7")
+    res = gpu_ctx.solve_batch([m, empty, m], opts(1e-12, max_iterations=55))
+    assert res[0].status == res[2].status == PdlpStatus.iteration_limit
+    assert res[0].iterations == res[2].iterations == 55
+    assert res[0].objective == res[2].objective
+    assert res[1].status == PdlpStatus.optimal and res[1].message == "trivial"
