@@ -112,7 +112,11 @@ typedef struct mc_pdlp_options {
                                          -1 = one thread per column over shared-memory
                                          tiles, 1..32 (power of two) = lanes per column */
     int32_t lanes_per_row;            /* A x kernel, same meaning per row */
-    int32_t reserved_i[5];
+    int32_t warm_start_guard;         /* 1: with a warm start, evaluate the reference's KKT score
+                                         of the warm start and of the cold start (x = proj(0),
+                                         y = 0) on the device and run from the better one; a
+                                         cold start also drops initial_primal_weight */
+    int32_t reserved_i[4];
     double reserved_d[8];
 } mc_pdlp_options;
 
@@ -152,7 +156,11 @@ typedef struct mc_pdlp_result {
     double kernel_ms_by_kind[MC_KERNEL_KINDS];
     int64_t launches_by_kind[MC_KERNEL_KINDS];
     int64_t kernel_launches;          /* engine kernels launched by this solve */
-    double reserved_d[4];
+    int32_t warm_start_used;          /* 1 if the solve started from the given warm start */
+    int32_t reserved_i0;
+    double warm_start_score;          /* guard: max(primal, dual, gap) at the warm start */
+    double cold_start_score;          /* guard: the same at the cold start */
+    double reserved_d[2];
 } mc_pdlp_result;
 
 /* Optional per-check history (one entry per restart check). */
@@ -227,6 +235,32 @@ int mc_pdlp_solve(const mc_lp* lp, const mc_pdlp_options* options,
 int mc_pdlp_ctx_solve_batch(mc_pdlp_ctx* ctx, const mc_lp* lps, int32_t count,
                             const mc_pdlp_options* options, double* const* primal_out,
                             double* const* dual_out, mc_pdlp_result* results);
+
+/*
+ * Learned warm start (no counterpart in the reference): a bipartite
+ * message-passing network over an LP's constraint/variable graph (hidden 64,
+ * `rounds` rounds, FP32) that predicts a primal/dual starting point and the
+ * log of the initial primal weight.  Trained and run on the GPU by the
+ * engine's own forward/backward kernels.  LPs are read from host memory.
+ * Feed the prediction to mc_pdlp_ctx_solve as initial_primal / initial_dual /
+ * initial_primal_weight with warm_start_guard = 1, which falls back to the
+ * cold start whenever the prediction's KKT score is worse.
+ */
+typedef struct mc_gnn mc_gnn;
+int mc_gnn_create(int device, int rounds, uint64_t seed, mc_gnn** out);
+int mc_gnn_destroy(mc_gnn* net);
+int mc_gnn_num_params(const mc_gnn* net, int64_t* count);
+int mc_gnn_get_params(mc_gnn* net, float* params_out);
+int mc_gnn_set_params(mc_gnn* net, const float* params_in);
+/* x_out[n], y_out[m] in the LP's original units; *log_omega_out (may be NULL) */
+int mc_gnn_predict(mc_gnn* net, const mc_lp* lp, double* x_out, double* y_out, double* log_omega_out);
+/* loss against a solved instance (x*, y*, log omega*) and its gradient
+ * (grad_out[num_params], may be NULL) */
+int mc_gnn_loss_and_grad(mc_gnn* net, const mc_lp* lp, const double* x_target, const double* y_target,
+                         double log_omega_target, double* loss, float* grad_out);
+/* one Adam step (beta 0.9 / 0.999) on one instance; *loss before the step */
+int mc_gnn_train_step(mc_gnn* net, const mc_lp* lp, const double* x_target, const double* y_target,
+                      double log_omega_target, float learning_rate, double* loss);
 
 /*
  * Kernel-level entry points (device pointers, the context's stream), used by

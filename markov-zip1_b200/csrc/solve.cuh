@@ -449,6 +449,40 @@ int run_chunks(Ctx& ctx, const E& eng, DevState* st, long long maxit, long long 
     return MC_OK;
 }
 
+// Start selection.  `start(warm)` writes the starting point and resets the
+// device state; `init()` finishes the engine-specific preparation.  With the
+// guard, the reference's KKT score (max of primal, dual, gap; pdlp.cpp:133)
+// of the warm start and of the cold start are evaluated on the device and the
+// solve runs from the smaller.
+template <class E, class Start, class Init>
+int choose_start(Ctx& ctx, const E& eng, DevState* st, const Controls& ctl, bool have_warm, bool guard,
+                 Start&& start, Init&& init, mc_pdlp_result* res) {
+    TRY(init());
+    res->warm_start_used = have_warm ? 1 : 0;
+    if (!have_warm || !guard) return MC_OK;
+    const TraceBuf none{0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    auto score = [&](double* out) -> int {
+        TRY(eng.check(ctx, 0, 1, ctl, none));
+        CU(cudaMemcpyAsync(&ctx.h_state[1], st, sizeof(DevState), cudaMemcpyDeviceToHost, ctx.stream));
+        CU(cudaStreamSynchronize(ctx.stream));
+        TRY(ctx.drain_profile());
+        *out = ctx.h_state[1].nonfinite ? INFINITY : ctx.h_state[1].score;
+        return MC_OK;
+    };
+    double sw = 0.0, s0 = 0.0;
+    TRY(score(&sw));
+    TRY(start(false));
+    TRY(init());
+    TRY(score(&s0));
+    const bool use_warm = sw < s0;
+    TRY(start(use_warm));
+    TRY(init());
+    res->warm_start_used = use_warm ? 1 : 0;
+    res->warm_start_score = sw;
+    res->cold_start_score = s0;
+    return MC_OK;
+}
+
 // ------------------------------------------------------------------ solve
 static void fill_message(mc_pdlp_result* r, const char* msg) {
     std::snprintf(r->message, sizeof r->message, "%s", msg);
@@ -660,18 +694,28 @@ int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* 
              ax_bar, dx, partials, st, o->ruiz_scaling ? o->ruiz_iterations : 0));
     const double obj_sign = (lp->objective_sense == MC_MAXIMIZE) ? -1.0 : 1.0;
     const int nbc = blocks_for(ctx, n, kBlock), nbr = blocks_for(ctx, m, kBlock);
-    ctx.begin_launch(MC_KERNEL_SETUP);
-    k_setup_cols<<<nbc, kBlock, 0, s>>>(n, csc_start, csc_val, in_obj, in_lo, in_hi, col_scale, d_warm_x, obj_sign,
-                                        c, lo, hi, c_orig, lo_orig, hi_orig, col_norm, x, x_avg, partials);
-    ctx.end_launch();
-    ctx.begin_launch(MC_KERNEL_SETUP);
-    k_setup_rows<<<nbr, kBlock, 0, s>>>(m, csr_start, csr_val, in_rlo, in_rhi, row_scale, d_warm_y, blo, bhi,
-                                        blo_orig, bhi_orig, row_norm, y, y_avg, partials);
-    ctx.end_launch();
-    ctx.begin_launch(MC_KERNEL_SETUP);
-    k_setup_scalars<<<1, 1024, 0, s>>>(partials, nbc, nbr, o->initial_primal_weight, o->step_size_reduction, st);
-    ctx.end_launch();
-    TRY(ctx.launch_check("setup"));
+    // starting point (pdlp.cpp:153-191): warm = the caller's warm start and
+    // primal weight, cold = x = proj(0), y = 0 and the derived weight
+    auto start = [&](bool warm) -> int {
+        ctx.begin_launch(MC_KERNEL_SETUP);
+        k_setup_cols<<<nbc, kBlock, 0, s>>>(n, csc_start, csc_val, in_obj, in_lo, in_hi, col_scale,
+                                            warm ? d_warm_x : nullptr, obj_sign, c, lo, hi, c_orig, lo_orig,
+                                            hi_orig, col_norm, x, x_avg, partials);
+        ctx.end_launch();
+        ctx.begin_launch(MC_KERNEL_SETUP);
+        k_setup_rows<<<nbr, kBlock, 0, s>>>(m, csr_start, csr_val, in_rlo, in_rhi, row_scale,
+                                            warm ? d_warm_y : nullptr, blo, bhi, blo_orig, bhi_orig, row_norm, y,
+                                            y_avg, partials);
+        ctx.end_launch();
+        ctx.begin_launch(MC_KERNEL_SETUP);
+        k_setup_scalars<<<1, 1024, 0, s>>>(partials, nbc, nbr,
+                                           (warm || !o->warm_start_guard) ? o->initial_primal_weight : 0.0,
+                                           o->step_size_reduction, st);
+        ctx.end_launch();
+        return ctx.launch_check("setup");
+    };
+    const bool have_warm = d_warm_x != nullptr || d_warm_y != nullptr;
+    TRY(start(have_warm));
 
     Original O{c_orig, in_obj, lo_orig, hi_orig, blo_orig, bhi_orig, col_scale, row_scale, lp->objective_offset};
     Controls ctl{o->primal_tolerance, o->dual_tolerance, o->gap_tolerance, o->restart_reduction_factor,
@@ -718,6 +762,7 @@ int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* 
                                    static_cast<int*>(at(o_col_bounds)), static_cast<int*>(at(o_row_bounds)));
         TRY(build_tiles(ctx, eng.pl, m, n, csc_start, csr_start, static_cast<int*>(at(o_col_bounds)),
                         static_cast<int*>(at(o_row_bounds)), chunk));
+        TRY(choose_start(ctx, eng, st, ctl, have_warm, o->warm_start_guard != 0, start, [] { return MC_OK; }, res));
         TRY(run_chunks(ctx, eng, st, o->max_iterations, o->restart_every, poll_every, ctl, tr));
     } else {
         EngineMixed eng;
@@ -753,8 +798,7 @@ int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* 
         ctx.begin_launch(MC_KERNEL_SETUP);
         k_to_float<<<nbr, kBlock, 0, s>>>(m, row_norm, f_rn);
         ctx.end_launch();
-        for (float* z : {f_x, f_xb, f_xa, f_dx}) CU(cudaMemsetAsync(z, 0, sizeof(float) * (size_t)n, s));
-        for (float* z : {f_y, f_ya, f_axb}) CU(cudaMemsetAsync(z, 0, sizeof(float) * (size_t)m, s));
+
         Iterates<float>& P = eng.P;
         P.m = m;
         P.n = n;
@@ -805,9 +849,14 @@ int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* 
         MC_DISPATCH_G(eng.pl.g_col, eng.nb_res_col = grid_for(ctx, k_residual_cols_mx<G>, n, kBlock / G));
         eng.nb_recenter = grid_for(ctx, k_recenter_mx, (long long)n + m, kBlock);
         eng.nb_apply = grid_for(ctx, k_dual_apply_mx, m, kBlock);
-        // first correction LP around the start point
-        TRY(eng.residual_pass(ctx));
-        TRY(eng.recenter(ctx, 1));
+        // the first correction LP around the start point (zero corrections)
+        auto init = [&]() -> int {
+            for (float* z : {f_x, f_xb, f_xa, f_dx}) CU(cudaMemsetAsync(z, 0, sizeof(float) * (size_t)n, s));
+            for (float* z : {f_y, f_ya, f_axb}) CU(cudaMemsetAsync(z, 0, sizeof(float) * (size_t)m, s));
+            TRY(eng.residual_pass(ctx));
+            return eng.recenter(ctx, 1);
+        };
+        TRY(choose_start(ctx, eng, st, ctl, have_warm, o->warm_start_guard != 0, start, init, res));
         TRY(run_chunks(ctx, eng, st, o->max_iterations, o->restart_every, poll_every, ctl, tr));
     }
     CU(cudaMemcpy(&ctx.h_state[2], st, sizeof(DevState), cudaMemcpyDeviceToHost));

@@ -84,6 +84,7 @@ class PdlpOptions:
     check_every_chunks: int = 1
     lanes_per_column: int = 0                      # SpMV tuning, 0 = chosen by line length
     lanes_per_row: int = 0
+    warm_start_guard: bool = False                 # run from the better of warm / cold start
     initial_primal: Optional[np.ndarray] = None   # warm start, original space
     initial_dual: Optional[np.ndarray] = None
 
@@ -137,6 +138,9 @@ def _result_from(r: _abi.McPdlpResult, x, y, trace=None) -> PdlpResult:
         refinement_rounds=r.refinement_rounds,
         inner_iterations=r.inner_iterations,
         kernel_launches=r.kernel_launches,
+        warm_start_used=bool(r.warm_start_used),
+        warm_start_score=r.warm_start_score,
+        cold_start_score=r.cold_start_score,
         launches_by_kind={n: r.launches_by_kind[i] for i, n in enumerate(_abi.KERNEL_KIND_NAMES)
                           if n != "-"},
         kernel_ms_by_kind={n: r.kernel_ms_by_kind[i] for i, n in enumerate(_abi.KERNEL_KIND_NAMES)

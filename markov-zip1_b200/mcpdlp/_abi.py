@@ -84,7 +84,8 @@ class McPdlpOptions(C.Structure):
         ("check_every_chunks", C.c_int32),
         ("lanes_per_column", C.c_int32),
         ("lanes_per_row", C.c_int32),
-        ("reserved_i", C.c_int32 * 5),
+        ("warm_start_guard", C.c_int32),
+        ("reserved_i", C.c_int32 * 4),
         ("reserved_d", C.c_double * 8),
     ]
 
@@ -113,7 +114,11 @@ class McPdlpResult(C.Structure):
         ("kernel_ms_by_kind", C.c_double * MC_KERNEL_KINDS),
         ("launches_by_kind", C.c_int64 * MC_KERNEL_KINDS),
         ("kernel_launches", C.c_int64),
-        ("reserved_d", C.c_double * 4),
+        ("warm_start_used", C.c_int32),
+        ("reserved_i0", C.c_int32),
+        ("warm_start_score", C.c_double),
+        ("cold_start_score", C.c_double),
+        ("reserved_d", C.c_double * 2),
     ]
 
 

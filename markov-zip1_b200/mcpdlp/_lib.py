@@ -53,6 +53,14 @@ ENGINE_SIGNATURES = {
     "mc_pdlp_ctx_solve": ([_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP], C.c_int),
     "mc_pdlp_solve": ([_VP, _VP, _VP, _VP, _VP, _VP, _VP], C.c_int),
     "mc_pdlp_ctx_solve_batch": ([_VP, _VP, C.c_int32, _VP, _VP, _VP, _VP], C.c_int),
+    "mc_gnn_create": ([C.c_int, C.c_int, C.c_uint64, _VP], C.c_int),
+    "mc_gnn_destroy": ([_VP], C.c_int),
+    "mc_gnn_num_params": ([_VP, _VP], C.c_int),
+    "mc_gnn_get_params": ([_VP, _VP], C.c_int),
+    "mc_gnn_set_params": ([_VP, _VP], C.c_int),
+    "mc_gnn_predict": ([_VP, _VP, _VP, _VP, _VP], C.c_int),
+    "mc_gnn_loss_and_grad": ([_VP, _VP, _VP, _VP, C.c_double, _VP, _VP], C.c_int),
+    "mc_gnn_train_step": ([_VP, _VP, _VP, _VP, C.c_double, C.c_float, _VP], C.c_int),
     "mc_spmv_csr": ([_VP, _I32, _I32, _VP, _VP, _VP, _VP, _VP], C.c_int),
     "mc_csc_to_csr": ([_VP, _I32, _I32, _I64, _VP, _VP, _VP, _VP, _VP, _VP], C.c_int),
     "mc_ruiz_equilibrate": ([_VP, _I32, _I32, _I64, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP,
