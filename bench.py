@@ -44,7 +44,15 @@ sys.path.insert(0, str(ROOT / "oracle"))
 
 METRIC = "time-to-1e-8 KKT & SpMV HBM GB/s: plain FP64 vs FP32+refine+warm-start PDLP"
 UNIT = "PDHG iterations/s (solve to 1e-8 relative KKT)"
-WORKLOAD = dict(m=2_000_000, n=5_000_000, k=8, seed=1)
+WORKLOADS = {
+    # synthetic LP with known optimum, FP64 values, int32 indices
+    "config1": dict(m=2_000_000, n=5_000_000, k=8, seed=1, family="standard",
+                    label="synthetic LP m=2M n=5M 8 nnz/col (40M nnz), FP64, Ruiz 10 passes, tolerance 1e-8"),
+    # precision stress: |a| log-uniform over six decades, 20% boxed columns
+    "config2": dict(m=1_000_000, n=3_000_000, k=10, seed=1, family="precision",
+                    label="precision-stress LP m=1M n=3M 10 nnz/col (30M nnz), |a| in [1e-3,1e3], tolerance 1e-8"),
+}
+WORKLOAD = dict(WORKLOADS["config1"])
 TOL = 1e-8
 
 
@@ -174,7 +182,7 @@ def sum_over_ranks(dist, value: float, device) -> float:
 def make_model(seed: int):
     from mcpdlp import generators
     w = WORKLOAD
-    return generators.random_lp(seed, w["m"], w["n"], w["k"])
+    return generators.random_lp(seed, w["m"], w["n"], w["k"], w["family"])
 
 
 def cpu_reference_sample(model, warmup_runs: int = 1, timed_runs: int = 1, iters: int = 40) -> dict:
@@ -203,7 +211,7 @@ def cpu_reference_sample(model, warmup_runs: int = 1, timed_runs: int = 1, iters
     setup = float(np.median(t_setup))
     per_iter = max(1e-9, (float(np.median(t_run)) - setup) / iters)
     return dict(value=1.0 / per_iter, unit=UNIT, cores=1, kind=kind,
-                sample=(f"reference solve_pdlp on the same 2M x 5M LP (40M nnz): "
+                sample=(f"reference solve_pdlp on the same LP ({WORKLOAD['label']}): "
                         f"{len(t_setup)} setup-only solves (max_iterations=0, {setup:.2f} s) and "
                         f"{len(t_run)} solves of {iters} iterations; steady rate = {iters} / "
                         f"(T_{iters} - T_0)"),
@@ -223,8 +231,7 @@ def run_reference_arm(args) -> None:
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": sample["ms_per_iteration"] * 40,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded generator, known optimum)", "impl": "reference",
-        "config": dict(workload="synthetic LP m=2M n=5M 8 nnz/col (40M nnz), FP64, Ruiz 10 passes, "
-                                "tolerance 1e-8", m=WORKLOAD["m"], n=WORKLOAD["n"],
+        "config": dict(workload=WORKLOAD["label"], m=WORKLOAD["m"], n=WORKLOAD["n"],
                        nnz=WORKLOAD["n"] * WORKLOAD["k"], seed=WORKLOAD["seed"],
                        step="40 PDHG iterations of the reference CPU PDLP (setup excluded)"),
         "cpu_baseline": {k: sample[k] for k in ("value", "unit", "cores", "kind", "sample")},
@@ -252,6 +259,57 @@ def run_ncu_case(args) -> None:
     print(json.dumps({"ncu_case": args.precision, "iterations": r.iterations,
                       "launches": r.extra["launches_by_kind"]}), flush=True)
     ctx.close()
+
+
+def run_batch_arm(args) -> None:
+    """Batched solves (one launch set for many LPs): part1 = 256 uneven LPs
+    (m ~ U[100,20000], n ~ U[2m,4m], 4-12 nnz/col), part2 = 512 node variants
+    of one LP (m=5000, n=15000, 8 nnz/col) with 1-10 bounds tightened; to 1e-6."""
+    import torch
+    import mcpdlp
+    from mcpdlp import PdlpOptions, generators
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = init_dist(world, "nccl")
+    if args.workload == "batch1":
+        models = generators.batch_part1(1 + rank, 256)
+        label = "256 uneven LPs (m~U[100,20000], n~U[2m,4m], k~U{4..12}), batched, tolerance 1e-6"
+    else:
+        _, models, _ = generators.batch_part2(1 + rank, 512)
+        label = "512 node variants of one LP (m=5000, n=15000, 8 nnz/col), batched, tolerance 1e-6"
+    ctx = mcpdlp.Context(local)
+    o = PdlpOptions(device=local)
+    o.set_tolerance(1e-6)
+    for _ in range(args.warmup):
+        ctx.solve_batch(models, o)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = None
+    for _ in range(args.steps):
+        res = ctx.solve_batch(models, o)
+    el = max_over_ranks(dist, time.perf_counter() - t0, dev)
+    lps = sum_over_ranks(dist, float(len(models) * args.steps), dev)
+    st = [r.status.name for r in res]
+    errs = [abs(r.objective - m.info["optimum"]) / abs(m.info["optimum"]) for r, m in zip(res, models)
+            if r.status.name == "optimal" and "optimum" in m.info and args.workload == "batch1"]
+    line = {"metric": "batched PDLP solves to 1e-6 relative KKT", "value": lps / el, "unit": "LPs/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": el * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generators)",
+            "config": dict(workload=label, lps=len(models), nnz=sum(m.nnz for m in models)),
+            "statuses": {k: st.count(k) for k in sorted(set(st))},
+            "max_iterations_in_batch": max(r.iterations for r in res),
+            "max_objective_rel_err_vs_analytic": max(errs) if errs else None,
+            "gpu_launches": res[0].extra["kernel_launches"] * args.steps}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def run_engine_arm(args) -> None:
@@ -381,8 +439,7 @@ def run_engine_arm(args) -> None:
         "warmup": args.warmup, "ms_per_step": t_max * 1e3 / max(1, args.steps),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded generator, known optimum)",
-        "config": dict(workload="synthetic LP m=2M n=5M 8 nnz/col (40M nnz), FP64, Ruiz 10 passes, "
-                                "tolerance 1e-8", m=m, n=n, nnz=nnz, seed=WORKLOAD["seed"],
+        "config": dict(workload=WORKLOAD["label"], m=m, n=n, nnz=nnz, seed=WORKLOAD["seed"],
                        step="one full PDLP solve to 1e-8 relative KKT (replica per rank)",
                        l2="inputs larger than L2 (960 MB of matrix per iteration)",
                        parallelism=f"replicas x{world}"),
@@ -421,8 +478,14 @@ def main() -> None:
                     help="run one short profiled solve of the workload (for ncu) and exit")
     ap.add_argument("--ncu-iterations", type=int, default=12)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32_refine"])
+    ap.add_argument("--workload", default="config1", choices=["config1", "config2", "batch1", "batch2"])
     args = ap.parse_args()
-    if args.ncu_case:
+    if args.workload in WORKLOADS:
+        WORKLOAD.clear()
+        WORKLOAD.update(WORKLOADS[args.workload])
+    if args.workload in ("batch1", "batch2"):
+        run_batch_arm(args)
+    elif args.ncu_case:
         run_ncu_case(args)
     elif args.impl == "reference":
         run_reference_arm(args)

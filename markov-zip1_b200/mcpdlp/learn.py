@@ -119,23 +119,54 @@ class WarmStartNet:
         self.params = z["params"]
 
 
-def solve_targets(ctx: Context, models: list, options: PdlpOptions, batch: int = 128) -> list:
+def b_scale(model: Model) -> float:
+    """max(1, |finite row bounds|_inf): the network's primal unit."""
+    s = 1.0
+    for a in (model.row_lower, model.row_upper):
+        f = a[np.isfinite(a)]
+        if len(f):
+            s = max(s, float(np.abs(f).max()))
+    return s
+
+
+def shaped_primal(model: Model, x: np.ndarray, margin: float = 0.05) -> np.ndarray:
+    """Training target for the primal: entries at a finite bound are pushed
+    `margin` (in units of |b|_inf) beyond it, so that the prediction lands
+    outside the box there and the engine's projection makes it exact.  The
+    reference's dual residual sums |x_j - proj(x_j - g_j)|^2 over all columns,
+    so exact bound values matter for a warm start to score well."""
+    t = x.copy()
+    tol = 1e-6 * b_scale(model)
+    m = margin * b_scale(model)
+    lo, hi = model.var_lower, model.var_upper
+    at_lo = np.isfinite(lo) & (x <= lo + tol)
+    at_hi = np.isfinite(hi) & (x >= hi - tol)
+    t[at_lo] = lo[at_lo] - m
+    t[at_hi] = hi[at_hi] + m
+    return t
+
+
+def solve_targets(ctx: Context, models: list, options: PdlpOptions, batch: int = 128,
+                  margin: float = 0.05) -> list:
     """GPU PDLP solutions of `models` (batched) as training targets."""
     out = []
     for s in range(0, len(models), batch):
         chunk = models[s:s + batch]
         for m, r in zip(chunk, ctx.solve_batch(chunk, options)):
-            out.append(Target(m, r.primal, r.dual, math.log(max(r.extra["final_primal_weight"], 1e-12)), r))
+            out.append(Target(m, shaped_primal(m, r.primal, margin) if margin > 0 else r.primal, r.dual,
+                              math.log(max(r.extra["final_primal_weight"], 1e-12)), r))
     return out
 
 
-def solve_warm(ctx: Context, net: WarmStartNet, model: Model, options: PdlpOptions) -> PdlpResult:
-    """Solve from the network's prediction, guarded by the engine."""
+def solve_warm(ctx: Context, net: WarmStartNet, model: Model, options: PdlpOptions,
+               guard: bool = True) -> PdlpResult:
+    """Solve from the network's prediction, guarded by the engine (guard=False
+    forces the prediction, for measuring what it does on its own)."""
     x, y, lw = net.predict(model)
     o = PdlpOptions(**{k: getattr(options, k) for k in options.__dataclass_fields__})
     o.initial_primal, o.initial_dual = x, y
     o.initial_primal_weight = float(min(max(math.exp(lw), 1e-6), 1e6))
-    o.warm_start_guard = True
+    o.warm_start_guard = guard
     return ctx.solve(model, o)
 
 
@@ -149,14 +180,21 @@ def main() -> None:
     ap.add_argument("--target-iterations", type=int, default=20000)
     ap.add_argument("--tol", type=float, default=1e-4)
     ap.add_argument("--max-iterations", type=int, default=100000)
+    ap.add_argument("--margin", type=float, default=0.05)
+    ap.add_argument("--size", type=int, nargs=2, default=[50, 500],
+                    help="suppliers and customers uniform in [lo, hi] (the workload: 50 500)")
     ap.add_argument("--out", default="")
     args = ap.parse_args()
     ctx = Context(0)
     t0 = time.time()
-    train_models = [generators.transport(seed) for seed in range(args.train)]
+    def family(seed):
+        S = generators.uniform_int(seed, 0, *args.size)
+        D = generators.uniform_int(seed, 1, *args.size)
+        return generators.transport(seed, S, D)
+    train_models = [family(seed) for seed in range(args.train)]
     topt = PdlpOptions(max_iterations=args.target_iterations)
     topt.set_tolerance(1e-8)
-    data = solve_targets(ctx, train_models, topt)
+    data = solve_targets(ctx, train_models, topt, margin=args.margin)
     t_data = time.time() - t0
     net = WarmStartNet(0, 3, 0)
     t0 = time.time()
@@ -168,12 +206,14 @@ def main() -> None:
     eopt.set_tolerance(args.tol)
     rows = []
     for seed in range(10_000_000, 10_000_000 + args.test):
-        m = generators.transport(seed)
+        m = family(seed)
         cold = ctx.solve(m, eopt)
         warm = solve_warm(ctx, net, m, eopt)
+        forced = solve_warm(ctx, net, m, eopt, guard=False)
         rows.append(dict(S=m.info["S"], D=m.info["D"], cold_it=cold.iterations, warm_it=warm.iterations,
                          cold_ms=cold.total_ms, warm_ms=warm.total_ms, cold_status=cold.status.name,
                          warm_status=warm.status.name, used=warm.extra["warm_start_used"],
+                         forced_it=forced.iterations, forced_status=forced.status.name,
                          warm_score=warm.extra["warm_start_score"], cold_score=warm.extra["cold_start_score"],
                          cold_kkt=max(cold.primal_infeasibility, cold.dual_infeasibility, cold.duality_gap),
                          warm_kkt=max(warm.primal_infeasibility, warm.dual_infeasibility, warm.duality_gap)))
@@ -184,6 +224,9 @@ def main() -> None:
                    warm_used=sum(r["used"] for r in rows),
                    mean_cold_it=float(np.mean([r["cold_it"] for r in rows])),
                    mean_warm_it=float(np.mean([r["warm_it"] for r in rows])),
+                   mean_forced_it=float(np.mean([r["forced_it"] for r in rows])),
+                   forced_optimal=sum(r["forced_status"] == "optimal" for r in rows),
+                   size=args.size,
                    mean_cold_ms=float(np.mean([r["cold_ms"] for r in rows])),
                    mean_warm_ms=float(np.mean([r["warm_ms"] for r in rows])),
                    median_start_score_ratio=float(np.median([r["warm_score"] / max(r["cold_score"], 1e-300)
