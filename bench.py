@@ -272,12 +272,18 @@ def run_batch_arm(args) -> None:
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     dist = init_dist(world, "nccl")
+    from mcpdlp.parallel import shard_by_nnz
+    # weak scaling: N ranks share a batch N times the single-GPU batch, sharded
+    # by nonzeros; a rank generates only the LPs of its shard
     if args.workload == "batch1":
-        models = generators.batch_part1(1 + rank, 256)
-        label = "256 uneven LPs (m~U[100,20000], n~U[2m,4m], k~U{4..12}), batched, tolerance 1e-6"
+        shapes = generators.batch_part1_shapes(1, 256 * world)
+        mine = shard_by_nnz([n * k for (_, n, k) in shapes], world)[rank]
+        models = generators.batch_part1(1, 256 * world, only=mine)
+        label = "256 uneven LPs per GPU (m~U[100,20000], n~U[2m,4m], k~U{4..12}), batched, tolerance 1e-6"
     else:
-        _, models, _ = generators.batch_part2(1 + rank, 512)
-        label = "512 node variants of one LP (m=5000, n=15000, 8 nnz/col), batched, tolerance 1e-6"
+        mine = shard_by_nnz([1] * (512 * world), world)[rank]
+        _, models, _ = generators.batch_part2(1, 512 * world, only=mine)
+        label = "512 node variants per GPU of one LP (m=5000, n=15000, 8 nnz/col), batched, tolerance 1e-6"
     ctx = mcpdlp.Context(local)
     o = PdlpOptions(device=local)
     o.set_tolerance(1e-6)

@@ -99,25 +99,33 @@ def tighten_bounds(base: Model, seed: int) -> tuple[Model, np.ndarray]:
     return v, cols[:cnt].copy()
 
 
-def batch_part1(seed: int, count: int = 256, m_range=(100, 20000)) -> list:
-    """Uneven batch: `count` LPs of the standard family with m ~ U[m_range],
-    n ~ U[2m, 4m], k ~ U{4..12} nonzeros per column (each from its own seed)."""
+def batch_part1_shapes(seed: int, count: int = 256, m_range=(100, 20000)) -> list:
+    """(m, n, k) of the uneven batch: m ~ U[m_range], n ~ U[2m, 4m], k ~ U{4..12}."""
     lib = _lib.lpgen()
     out = []
     for b in range(count):
         m = int(lib.lpgen_uniform_int(seed, 3 * b, m_range[0], m_range[1]))
         n = int(lib.lpgen_uniform_int(seed, 3 * b + 1, 2 * m, 4 * m))
         k = int(lib.lpgen_uniform_int(seed, 3 * b + 2, 4, 12))
-        out.append(random_lp(seed * 100003 + b, m, n, k))
+        out.append((m, n, k))
     return out
 
 
-def batch_part2(seed: int, variants: int = 512, m: int = 5000, n: int = 15000, k: int = 8):
+def batch_part1(seed: int, count: int = 256, m_range=(100, 20000), only=None) -> list:
+    """Uneven batch: `count` LPs of the standard family with shapes from
+    batch_part1_shapes (each from its own seed); `only` selects indices."""
+    shapes = batch_part1_shapes(seed, count, m_range)
+    idx = range(count) if only is None else only
+    return [random_lp(seed * 100003 + b, *shapes[b]) for b in idx]
+
+
+def batch_part2(seed: int, variants: int = 512, m: int = 5000, n: int = 15000, k: int = 8, only=None):
     """One base LP and `variants` node variants (1-10 bounds tightened to
-    floor/ceil of x* -+ U(0,1)); returns (base, [variants], [tightened cols])."""
+    floor/ceil of x* -+ U(0,1)); returns (base, [variants], [tightened cols]);
+    `only` selects variant indices."""
     base = random_lp(seed, m, n, k)
     vs, cols = [], []
-    for v in range(variants):
+    for v in (range(variants) if only is None else only):
         mv, cv = tighten_bounds(base, seed * 7919 + v)
         vs.append(mv)
         cols.append(cv)
