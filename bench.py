@@ -196,6 +196,38 @@ def cpu_reference_sample(model, warmup_runs: int = 1, timed_runs: int = 1, iters
         solver, kind = OraclePort(), "port"
     o = _abi.default_options_struct()
     o.primal_tolerance = o.dual_tolerance = o.gap_tolerance = TOL
+    # the reference PDLP is single-threaded: pin it to one core for the sample
+    saved = os.sched_getaffinity(0) if hasattr(os, "sched_getaffinity") else None
+    if saved:
+        os.sched_setaffinity(0, {max(saved)})
+    try:
+        t_setup, t_run, r = _time_cpu_solves(solver, model, o, warmup_runs, timed_runs, iters)
+    finally:
+        if saved:
+            os.sched_setaffinity(0, saved)
+    setup = float(np.median(t_setup))
+    per_iter = max(1e-9, (float(np.median(t_run)) - setup) / iters)
+    return dict(value=1.0 / per_iter, unit=UNIT, cores=1, kind=kind,
+                sample=(f"reference solve_pdlp on the same LP ({WORKLOAD['label']}): "
+                        f"{len(t_setup)} setup-only solves (max_iterations=0, {setup:.2f} s) and "
+                        f"{len(t_run)} solves of {iters} iterations; steady rate = {iters} / "
+                        f"(T_{iters} - T_0); one pinned core of {host_cpu()}"),
+                setup_s=setup, ms_per_iteration=per_iter * 1e3, last_primal=r.primal_infeasibility)
+
+
+def host_cpu() -> str:
+    model = "unknown CPU"
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return f"{model} ({os.cpu_count()} logical cores on the host)"
+
+
+def _time_cpu_solves(solver, model, o, warmup_runs: int, timed_runs: int, iters: int):
     t_setup = []
     for _ in range(max(1, warmup_runs)):
         o.max_iterations = 0
@@ -208,14 +240,7 @@ def cpu_reference_sample(model, warmup_runs: int = 1, timed_runs: int = 1, iters
         t0 = time.perf_counter()
         r = solver.solve(model, o)
         t_run.append(time.perf_counter() - t0)
-    setup = float(np.median(t_setup))
-    per_iter = max(1e-9, (float(np.median(t_run)) - setup) / iters)
-    return dict(value=1.0 / per_iter, unit=UNIT, cores=1, kind=kind,
-                sample=(f"reference solve_pdlp on the same LP ({WORKLOAD['label']}): "
-                        f"{len(t_setup)} setup-only solves (max_iterations=0, {setup:.2f} s) and "
-                        f"{len(t_run)} solves of {iters} iterations; steady rate = {iters} / "
-                        f"(T_{iters} - T_0)"),
-                setup_s=setup, ms_per_iteration=per_iter * 1e3, last_primal=r.primal_infeasibility)
+    return t_setup, t_run, r
 
 
 def run_reference_arm(args) -> None:

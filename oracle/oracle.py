@@ -177,6 +177,8 @@ class ReferencePdlp:
         lib.ref_mps_fetch.restype = C.c_int
         lib.ref_last_error.argtypes = [C.c_char_p, C.c_size_t]
         lib.ref_last_error.restype = C.c_int
+        lib.ref_simplex_solve.argtypes = [_VP, C.c_int64, _VP, _VP, _VP, _VP]
+        lib.ref_simplex_solve.restype = C.c_int
         self.lib = lib
 
     def _err(self) -> str:
@@ -212,6 +214,25 @@ class ReferencePdlp:
         return dict(value=v, objective=obj, var_lower=vl, var_upper=vu, row_lower=rl,
                     row_upper=ru, row_scale=rs, col_scale=cs, iterations=it.value,
                     converged=bool(conv.value))
+
+    SIMPLEX_STATUS = ("optimal", "infeasible", "unbounded", "iteration_limit", "invalid_model",
+                      "invalid_options", "resource_limit", "numerical_failure")
+
+    def simplex(self, model: Model, iteration_limit: int = 0) -> dict:
+        """The reference's primal simplex (src/lp/reference/revised_simplex.cpp)
+        on a small LP, through the CLI's canonical path: the FP64 optimum of
+        LPs the simplex's dense limits admit (canonical rows <= 1024)."""
+        lp = model.to_struct()
+        x = np.zeros(model.num_cols)
+        obj = C.c_double(np.nan)
+        st = C.c_int32(-1)
+        it = C.c_int64(0)
+        rc = self.lib.ref_simplex_solve(C.addressof(lp), iteration_limit, _ptr(x), C.addressof(obj),
+                                        C.addressof(st), C.addressof(it))
+        if rc != 0:
+            raise RuntimeError(f"reference simplex threw: {self._err()}")
+        return dict(status=self.SIMPLEX_STATUS[st.value], objective=obj.value, primal=x,
+                    iterations=it.value)
 
     def verify_primal(self, model: Model, primal: np.ndarray, claimed: float, tol: float):
         lp = model.to_struct()

@@ -7,14 +7,17 @@
 //   lp::first_order::solve_pdlp      src/lp/first_order/pdlp.cpp:139
 //   scale::equilibrate_model         src/scale/ruiz_scaling.cpp:152
 //   verify::verify_primal            src/verify/primal_verifier.cpp:44
+//   lp::reference::solve (simplex)   src/lp/reference/revised_simplex.cpp (small LPs only)
 //   io::parse_mps                    src/io/mps.cpp:96 (fixture generation)
 // Only tests, the golden-fixture script and bench.py's reference arm use it.
 #include "mc_pdlp.h"
 
 #include "markov_cero/io/mps.hpp"
 #include "markov_cero/lp/first_order/pdlp.hpp"
+#include "markov_cero/lp/reference/revised_simplex.hpp"
 #include "markov_cero/model/model.hpp"
 #include "markov_cero/scale/ruiz_scaling.hpp"
+#include "markov_cero/transform/sparse_canonical_model.hpp"
 #include "markov_cero/verify/primal_verifier.hpp"
 
 #include <cmath>
@@ -190,6 +193,37 @@ int ref_verify_primal(const mc_lp* lp, const double* primal, double claimed_obje
         *max_row_violation = rep.maximum_row_violation;
         *max_var_violation = rep.maximum_variable_violation;
         *recomputed_objective = rep.recomputed_objective;
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return 1;
+    }
+}
+
+// The reference's primal simplex on a small LP, along the CLI's path without
+// presolve or scaling (apps/markov_cero_solve.cpp:275-276, :311, :332,
+// :393-394): sparse_canonicalize -> to_dense -> lp::reference::solve ->
+// reconstruct_primal / reconstruct_objective.  The simplex keeps its own
+// limits (src/lp/reference/revised_simplex.cpp:15-17, :252-257): a model past
+// them returns 1 with the reference's length_error message.
+// status: the reference's SolveStatus order (optimal 0, infeasible 1,
+// unbounded 2, iteration_limit 3, ...).
+int ref_simplex_solve(const mc_lp* lp, int64_t iteration_limit, double* primal_out,
+                      double* objective_out, int32_t* status, int64_t* iterations) {
+    try {
+        const mdl::Model model = to_model(lp);
+        const auto sparse = markov_cero::transform::sparse_canonicalize(model, /*relax_integrality=*/true);
+        const auto dense = sparse.to_dense();
+        markov_cero::lp::reference::Options ro;
+        if (iteration_limit > 0) ro.iteration_limit = static_cast<std::size_t>(iteration_limit);
+        const auto res = markov_cero::lp::reference::solve(dense, ro);
+        *status = static_cast<int32_t>(res.status);
+        *iterations = static_cast<int64_t>(res.phase_one_iterations + res.phase_two_iterations);
+        if (res.status == markov_cero::lp::reference::SolveStatus::optimal) {
+            const auto x = markov_cero::transform::reconstruct_primal(sparse, res.primal);
+            if (primal_out) std::memcpy(primal_out, x.data(), x.size() * sizeof(double));
+            *objective_out = markov_cero::transform::reconstruct_objective(sparse, res.objective);
+        }
         return 0;
     } catch (const std::exception& e) {
         g_error = e.what();

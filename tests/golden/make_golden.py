@@ -15,7 +15,12 @@ Writes, next to this script:
                    iterations, objective, residuals, SHA-256 of the primal and
                    dual bytes) at 1e-4 and 1e-8, the same for seeded synthetic
                    LPs (regenerated from their seed, pinned by a SHA-256 of the
-                   generated arrays), and equilibrate_model digests.
+                   generated arrays), equilibrate_model digests, and the
+                   reference primal simplex's optimum of small seeded
+                   transportation LPs (the FP64 optimum of that family, which
+                   has no analytic one).
+
+    python tests/golden/make_golden.py --only simplex   # refresh that section
 """
 from __future__ import annotations
 
@@ -45,6 +50,9 @@ SYNTHETIC = [  # (name, seed, m, n, k, family)
     ("precision_s1", 1, 300, 900, 10, "precision"),
 ]
 TOLS = [1e-4, 1e-8]
+TRANSPORT = [  # (seed, suppliers, customers): within the simplex's dense limits
+    (1, 20, 30), (2, 20, 30), (3, 25, 35), (4, 30, 40), (5, 40, 50), (6, 40, 60),
+]
 
 
 def sha(*arrays) -> str:
@@ -101,9 +109,30 @@ def record(ref, m: Model) -> dict:
     return out
 
 
+def simplex_section(ref) -> dict:
+    out = {}
+    for seed, S, D in TRANSPORT:
+        m = generators.transport(seed, S, D)
+        r = ref.simplex(m)
+        p = ref.solve(m, opts(1e-8))
+        out[f"transport_{seed}_{S}x{D}"] = dict(seed=seed, suppliers=S, customers=D,
+                                                digest=model_digest(m), status=r["status"],
+                                                objective=r["objective"],
+                                                iterations=r["iterations"],
+                                                pdlp_1e8=dict(status=p.status, iterations=p.iterations,
+                                                              objective=p.objective))
+        print("simplex", seed, S, D, r["status"], r["objective"], "pdlp", p.status, p.iterations)
+    return out
+
+
 def main() -> None:
     orc.build(reference=True)
     ref = orc.ReferencePdlp()
+    if "--only" in sys.argv and sys.argv[sys.argv.index("--only") + 1] == "simplex":
+        golden = json.loads((HERE / "golden.json").read_text())
+        golden["simplex"] = simplex_section(ref)
+        (HERE / "golden.json").write_text(json.dumps(golden, indent=1, sort_keys=True))
+        return
     golden = {"models": {}, "synthetic": {}, "ruiz": {}}
     fixtures = [blend_lp(), equality_lp(), ref.parse_mps(REF / "examples/phase3/tiny_simplex.mps")]
     fixtures[2].name = "tiny_simplex"
@@ -130,6 +159,7 @@ def main() -> None:
                                     scales_sha256=sha(e["row_scale"], e["col_scale"]),
                                     bounds_sha256=sha(e["objective"], e["var_lower"], e["var_upper"],
                                                       e["row_lower"], e["row_upper"]))
+    golden["simplex"] = simplex_section(ref)
     (HERE / "golden.json").write_text(json.dumps(golden, indent=1, sort_keys=True))
 
 

@@ -185,3 +185,39 @@ def test_reference_verifier_accepts_oracle_solution(oracle, reference):
     r = oracle.solve(m, options(1e-4))
     rep = reference.verify_primal(m, r.primal, r.objective, 1e-4)
     assert rep["passed"]
+
+
+# ------------------------------------------------- primal simplex optimum
+SIMPLEX = GOLDEN["simplex"]
+
+
+def transport_case(name: str) -> Model:
+    g = SIMPLEX[name]
+    return generators.transport(g["seed"], g["suppliers"], g["customers"])
+
+
+@pytest.mark.parametrize("name", list(SIMPLEX))
+def test_transport_generator_is_pinned(name):
+    m = transport_case(name)
+    assert sha(m.col_start, m.row_index, m.value, m.objective, m.var_lower, m.var_upper,
+               m.row_lower, m.row_upper) == SIMPLEX[name]["digest"]
+
+
+@pytest.mark.parametrize("name", ["transport_2_20x30", "transport_4_30x40"])
+def test_reference_simplex_reproduces_golden(reference, name):
+    r = reference.simplex(transport_case(name))
+    assert r["status"] == SIMPLEX[name]["status"] == "optimal"
+    assert r["objective"] == SIMPLEX[name]["objective"]
+
+
+@pytest.mark.parametrize("name", list(SIMPLEX))
+def test_oracle_pdlp_against_simplex_optimum(oracle, name):
+    """The reference PDLP at 1e-8 (restated) against the simplex's FP64
+    optimum: where it converges, within 1e-6 relative (src/lp/reference/
+    revised_simplex.cpp is the FP64 optimum of the transportation family)."""
+    g = SIMPLEX[name]
+    r = oracle.solve(transport_case(name), options(1e-8))
+    assert (r.status, r.iterations, r.objective) == (g["pdlp_1e8"]["status"], g["pdlp_1e8"]["iterations"],
+                                                     g["pdlp_1e8"]["objective"])
+    if r.status == 0:
+        assert abs(r.objective - g["objective"]) <= 1e-6 * abs(g["objective"])
