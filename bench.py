@@ -83,7 +83,7 @@ def kernel_bytes(kind: str, m: int, n: int, nnz: int, fp: int = 8) -> float:
 def ncu_traffic(kernel: str):
     """dram bytes per launch from the committed ncu summary, if any."""
     f = ROOT / "profiles" / "traffic_config1.txt"
-    if not f.exists():
+    if WORKLOAD["label"] != WORKLOADS["config1"]["label"] or not f.exists():
         return None
     for line in f.read_text().splitlines():
         parts = line.split()
@@ -310,30 +310,45 @@ def run_batch_arm(args) -> None:
         _, models, _ = generators.batch_part2(1, 512 * world, only=mine)
         label = "512 node variants per GPU of one LP (m=5000, n=15000, 8 nnz/col), batched, tolerance 1e-6"
     ctx = mcpdlp.Context(local)
-    o = PdlpOptions(device=local)
-    o.set_tolerance(1e-6)
-    for _ in range(args.warmup):
-        ctx.solve_batch(models, o)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    res = None
-    for _ in range(args.steps):
-        res = ctx.solve_batch(models, o)
-    el = max_over_ranks(dist, time.perf_counter() - t0, dev)
+    from mcpdlp import Precision
+
+    def timed(precision):
+        o = PdlpOptions(device=local, precision=precision)
+        o.set_tolerance(1e-6)
+        for _ in range(args.warmup):
+            ctx.solve_batch(models, o)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = None
+        for _ in range(args.steps):
+            res = ctx.solve_batch(models, o)
+        return max_over_ranks(dist, time.perf_counter() - t0, dev), res
+
+    # the FP32 + FP64-refinement form is the workload's; plain FP64 beside it
+    el, res = timed(Precision.fp32_refine)
+    el64, res64 = timed(Precision.fp64)
     lps = sum_over_ranks(dist, float(len(models) * args.steps), dev)
-    st = [r.status.name for r in res]
-    errs = [abs(r.objective - m.info["optimum"]) / abs(m.info["optimum"]) for r, m in zip(res, models)
-            if r.status.name == "optimal" and "optimum" in m.info and args.workload == "batch1"]
+
+    def summary(rs):
+        st = [r.status.name for r in rs]
+        errs = [abs(r.objective - m.info["optimum"]) / abs(m.info["optimum"]) for r, m in zip(rs, models)
+                if r.status.name == "optimal" and "optimum" in m.info and args.workload == "batch1"]
+        return {"statuses": {k: st.count(k) for k in sorted(set(st))},
+                "max_iterations_in_batch": max(r.iterations for r in rs),
+                "max_objective_rel_err_vs_analytic": max(errs) if errs else None}
+
     line = {"metric": "batched PDLP solves to 1e-6 relative KKT", "value": lps / el, "unit": "LPs/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": el * 1e3 / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic (seeded generators)",
-            "config": dict(workload=label, lps=len(models), nnz=sum(m.nnz for m in models)),
-            "statuses": {k: st.count(k) for k in sorted(set(st))},
-            "max_iterations_in_batch": max(r.iterations for r in res),
-            "max_objective_rel_err_vs_analytic": max(errs) if errs else None,
+            "config": dict(workload=label, lps=len(models), nnz=sum(m.nnz for m in models),
+                           form="FP32 PDHG + FP64 residuals/restarts/refinement, packed CSR, CUDA graph"),
+            **summary(res),
+            "forms": {"fp32_refine": {"LPs_per_s": lps / el, "ms_per_step": el * 1e3 / args.steps},
+                      "fp64": {"LPs_per_s": lps / el64, "ms_per_step": el64 * 1e3 / args.steps,
+                               **summary(res64)}},
             "gpu_launches": res[0].extra["kernel_launches"] * args.steps}
     if rank == 0:
         print(json.dumps(line), flush=True)

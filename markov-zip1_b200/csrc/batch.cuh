@@ -4,67 +4,236 @@
 #include "batch_kernels.cuh"
 #include "solve.cuh"
 
+#include <tuple>
 #include <vector>
 
 namespace mc {
 
-struct EngineBatch {
-    Iterates<double> P;
-    Original O;
+// What both batched engines share: the work queue and the lanes.
+struct BatchCommon {
     BatchRefs B;
     DevState* global = nullptr;  // poll flag: every LP done
+    int* active = nullptr;       // the work queue (B.active, writable)
+    int* active_count = nullptr;
     int g_col = 1, g_row = 1;
+
+    // persistent grids: one wave of resident blocks, at most one per tile
+    template <class K>
+    static int grid(const Ctx& ctx, K kernel, int tiles) { return grid_for(ctx, kernel, tiles, 1); }
+
+    int compact(Ctx& ctx) const {
+        ctx.begin_launch(MC_KERNEL_OTHER);
+        kb_compact<<<1, kCompactThreads, 0, ctx.stream>>>(B, active, active_count, global);
+        ctx.end_launch();
+        return MC_OK;
+    }
+};
+
+// FP64 batched PDHG.
+struct EngineBatch : BatchCommon {
+    Iterates<double> P;
+    Original O;
+
+    int primal(Ctx& ctx, int g, bool step, int k) const {
+        cudaStream_t s = ctx.stream;
+        const int nc = B.cols.ntiles;
+        ctx.begin_launch(MC_KERNEL_PRIMAL);
+        if (step) {
+            MC_DISPATCH_G(g, (kb_primal<G, true, double><<<grid(ctx, kb_primal<G, true, double>, nc), kBlock, 0, s>>>(P, B, k)));
+        } else {
+            MC_DISPATCH_G(g, (kb_primal<G, false, double><<<grid(ctx, kb_primal<G, false, double>, nc), kBlock, 0, s>>>(P, B, k)));
+        }
+        ctx.end_launch();
+        return MC_OK;
+    }
+
+    int dual(Ctx& ctx, int g, int k) const {
+        cudaStream_t s = ctx.stream;
+        ctx.begin_launch(MC_KERNEL_DUAL);
+        MC_DISPATCH_G(g, (kb_dual<G><<<grid(ctx, kb_dual<G>, B.rows.ntiles), kBlock, 0, s>>>(P, B, k)));
+        ctx.end_launch();
+        return MC_OK;
+    }
 
     int iteration(Ctx& ctx, int k, bool step, const Controls& ctl) const {
         cudaStream_t s = ctx.stream;
-        const int nc = B.cols.ntiles, nr = B.rows.ntiles;
-        ctx.begin_launch(MC_KERNEL_PRIMAL);
-        if (step) {
-            MC_DISPATCH_G(g_col, (kb_primal<G, true><<<nc, kBlock, 0, s>>>(P, B, k)));
-        } else {
-            MC_DISPATCH_G(g_col, (kb_primal<G, false><<<nc, kBlock, 0, s>>>(P, B, k)));
-        }
-        ctx.end_launch();
+        const int nr = B.rows.ntiles;
+        TRY(primal(ctx, g_col, step, k));
         if (step) {
             ctx.begin_launch(MC_KERNEL_DUAL_STEP);
-            MC_DISPATCH_G(g_row, (kb_dual_probe<G><<<nr, kBlock, 0, s>>>(P, B)));
+            MC_DISPATCH_G(probe_lanes(g_row), (kb_dual_probe<G, double><<<grid(ctx, kb_dual_probe<G, double>, nr), kBlock, 0, s>>>(P, B)));
             ctx.end_launch();
             ctx.begin_launch(MC_KERNEL_OTHER);
             kb_step_size<<<B.nlp, 256, 0, s>>>(P.partials, B, ctl);
             ctx.end_launch();
             ctx.begin_launch(MC_KERNEL_DUAL_STEP);
-            kb_dual_apply<<<nr, kBlock, 0, s>>>(P, B, k);
+            kb_dual_apply<<<grid(ctx, kb_dual_apply, nr), kBlock, 0, s>>>(P, B, k);
             ctx.end_launch();
         } else {
-            ctx.begin_launch(MC_KERNEL_DUAL);
-            MC_DISPATCH_G(g_row, (kb_dual<G><<<nr, kBlock, 0, s>>>(P, B, k)));
-            ctx.end_launch();
+            TRY(dual(ctx, g_row, k));
         }
         return ctx.launch_check("batch iteration");
     }
 
     int check(Ctx& ctx, long long span, int final_pass, const Controls& ctl, const TraceBuf&) const {
         cudaStream_t s = ctx.stream;
+        const int nc = B.cols.ntiles, nr = B.rows.ntiles;
         ctx.begin_launch(MC_KERNEL_RESIDUAL);
-        MC_DISPATCH_G(g_row, (kb_residual_rows<G><<<B.rows.ntiles, kBlock, 0, s>>>(P, O, B)));
+        MC_DISPATCH_G(g_row, (kb_residual_rows<G><<<grid(ctx, kb_residual_rows<G>, nr), kBlock, 0, s>>>(P, O, B)));
         ctx.end_launch();
         ctx.begin_launch(MC_KERNEL_RESIDUAL);
-        MC_DISPATCH_G(g_col, (kb_residual_cols<G><<<B.cols.ntiles, kBlock, 0, s>>>(P, O, B)));
+        MC_DISPATCH_G(g_col, (kb_residual_cols<G><<<grid(ctx, kb_residual_cols<G>, nc), kBlock, 0, s>>>(P, O, B)));
         ctx.end_launch();
         ctx.begin_launch(MC_KERNEL_RESIDUAL);
         kb_finalize<<<B.nlp, 256, 0, s>>>(P.partials, B, span, final_pass, ctl);
         ctx.end_launch();
         if (!final_pass) {
             ctx.begin_launch(MC_KERNEL_OTHER);
-            kb_restart_copy<<<B.cols.ntiles + B.rows.ntiles, kBlock, 0, s>>>(P, B);
+            kb_restart_copy<<<grid(ctx, kb_restart_copy, nc + nr), kBlock, 0, s>>>(P, B);
             ctx.end_launch();
         }
-        ctx.begin_launch(MC_KERNEL_OTHER);
-        kb_all_done<<<1, 256, 0, s>>>(B.st, B.nlp, global);
-        ctx.end_launch();
+        TRY(compact(ctx));
         return ctx.launch_check("batch check");
     }
 };
+
+// FP32 + FP64-refinement batched PDHG (the mixed form of solve.cuh, per LP).
+struct EngineBatchMixed : BatchCommon {
+    Iterates<float> P;
+    MixedState M;
+    Original O;
+
+    int primal(Ctx& ctx, int g, bool step, int k) const {
+        cudaStream_t s = ctx.stream;
+        const int nc = B.cols.ntiles;
+        ctx.begin_launch(MC_KERNEL_PRIMAL);
+        if (step) {
+            MC_DISPATCH_G(g, (kb_primal<G, true, float><<<grid(ctx, kb_primal<G, true, float>, nc), kBlock, 0, s>>>(P, B, k)));
+        } else {
+            MC_DISPATCH_G(g, (kb_primal<G, false, float><<<grid(ctx, kb_primal<G, false, float>, nc), kBlock, 0, s>>>(P, B, k)));
+        }
+        ctx.end_launch();
+        return MC_OK;
+    }
+
+    int dual(Ctx& ctx, int g, int k) const {
+        cudaStream_t s = ctx.stream;
+        ctx.begin_launch(MC_KERNEL_DUAL);
+        MC_DISPATCH_G(g, (kb_dual_mx<G><<<grid(ctx, kb_dual_mx<G>, B.rows.ntiles), kBlock, 0, s>>>(P, M, B, k)));
+        ctx.end_launch();
+        return MC_OK;
+    }
+
+    int residual_pass(Ctx& ctx) const {
+        cudaStream_t s = ctx.stream;
+        const int nc = B.cols.ntiles, nr = B.rows.ntiles;
+        ctx.begin_launch(MC_KERNEL_RESIDUAL);
+        MC_DISPATCH_G(g_row, (kb_residual_rows_mx<G><<<grid(ctx, kb_residual_rows_mx<G>, nr), kBlock, 0, s>>>(P, M, O, B)));
+        ctx.end_launch();
+        ctx.begin_launch(MC_KERNEL_RESIDUAL);
+        MC_DISPATCH_G(g_col, (kb_residual_cols_mx<G><<<grid(ctx, kb_residual_cols_mx<G>, nc), kBlock, 0, s>>>(P, M, O, B)));
+        ctx.end_launch();
+        return ctx.launch_check("batch residual (mixed)");
+    }
+
+    int recenter(Ctx& ctx, int force) const {
+        ctx.begin_launch(MC_KERNEL_OTHER);
+        kb_recenter_mx<<<grid(ctx, kb_recenter_mx, B.cols.ntiles + B.rows.ntiles), kBlock, 0, ctx.stream>>>(P, M, B,
+                                                                                                          force);
+        ctx.end_launch();
+        return ctx.launch_check("batch recenter (mixed)");
+    }
+
+    int iteration(Ctx& ctx, int k, bool step, const Controls& ctl) const {
+        cudaStream_t s = ctx.stream;
+        const int nr = B.rows.ntiles;
+        TRY(primal(ctx, g_col, step, k));
+        if (step) {
+            ctx.begin_launch(MC_KERNEL_DUAL_STEP);
+            MC_DISPATCH_G(probe_lanes(g_row), (kb_dual_probe<G, float><<<grid(ctx, kb_dual_probe<G, float>, nr), kBlock, 0, s>>>(P, B)));
+            ctx.end_launch();
+            ctx.begin_launch(MC_KERNEL_OTHER);
+            kb_step_size<<<B.nlp, 256, 0, s>>>(P.partials, B, ctl);
+            ctx.end_launch();
+            ctx.begin_launch(MC_KERNEL_DUAL_STEP);
+            kb_dual_apply_mx<<<grid(ctx, kb_dual_apply_mx, nr), kBlock, 0, s>>>(P, M, B, k);
+            ctx.end_launch();
+        } else {
+            TRY(dual(ctx, g_row, k));
+        }
+        return ctx.launch_check("batch iteration (mixed)");
+    }
+
+    int check(Ctx& ctx, long long span, int final_pass, const Controls& ctl, const TraceBuf&) const {
+        TRY(residual_pass(ctx));
+        ctx.begin_launch(MC_KERNEL_RESIDUAL);
+        kb_finalize<<<B.nlp, 256, 0, ctx.stream>>>(P.partials, B, span, final_pass, ctl);
+        ctx.end_launch();
+        if (!final_pass) TRY(recenter(ctx, 0));
+        TRY(compact(ctx));
+        return ctx.launch_check("batch check (mixed)");
+    }
+};
+
+// The lanes autotuner: lanes per column for the A^T y kernel and lanes per
+// row for the A x kernel, each chosen by timing that kernel over the batch
+// itself at every power of two 1..32 (best of two timed launches after a
+// warm one).  It runs from the start iterate, which is saved first and put
+// back after, so the solve that follows is the one the chosen lanes give.
+// The choice is kept per context, batch shape and precision: later solves of
+// the same shape reuse it (and repeat bit-identically).
+template <class E>
+int tune_lanes(Ctx& ctx, E& eng, int precision, void* const save_n[3], void* const save_m[2]) {
+    const auto key = std::make_tuple((long long)eng.P.n, (long long)eng.P.m, (long long)eng.B.nlp,
+                                     (long long)eng.B.cols.ntiles * 4 + precision, (long long)eng.B.rows.ntiles);
+    auto hit = ctx.lane_cache.find(key);
+    if (hit != ctx.lane_cache.end()) {
+        eng.g_col = hit->second.first;
+        eng.g_row = hit->second.second;
+        return MC_OK;
+    }
+    cudaStream_t s = ctx.stream;
+    const size_t elem = sizeof(*eng.P.x);
+    const size_t bn = elem * (size_t)eng.P.n, bm = elem * (size_t)eng.P.m;
+    void* const cur_n[3] = {eng.P.x, eng.P.x_bar, eng.P.x_avg};
+    void* const cur_m[2] = {eng.P.y, eng.P.y_avg};
+    for (int q = 0; q < 3; ++q) CU(cudaMemcpyAsync(save_n[q], cur_n[q], bn, cudaMemcpyDeviceToDevice, s));
+    for (int q = 0; q < 2; ++q) CU(cudaMemcpyAsync(save_m[q], cur_m[q], bm, cudaMemcpyDeviceToDevice, s));
+    auto ok = [](cudaError_t e, const char* what) { return e == cudaSuccess ? MC_OK : cuda_fail(e, what, __LINE__); };
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CU(cudaEventCreate(&e0));
+    int rc = ok(cudaEventCreate(&e1), "cudaEventCreate");
+    float best[2] = {3.0e38f, 3.0e38f};
+    int pick[2] = {eng.g_col, eng.g_row};
+    for (int g = 1; g <= 32 && rc == MC_OK; g *= 2) {
+        for (int which = 0; which < 2 && rc == MC_OK; ++which) {
+            float t_min = 3.0e38f;
+            for (int rep = 0; rep < 3 && rc == MC_OK; ++rep) {
+                float ms = 0.f;
+                rc = ok(cudaEventRecord(e0, s), "cudaEventRecord");
+                if (rc == MC_OK) rc = which ? eng.dual(ctx, g, 0) : eng.primal(ctx, g, false, 0);
+                if (rc == MC_OK) rc = ctx.launch_check("lanes autotuner");
+                if (rc == MC_OK) rc = ok(cudaEventRecord(e1, s), "cudaEventRecord");
+                if (rc == MC_OK) rc = ok(cudaEventSynchronize(e1), "cudaEventSynchronize");
+                if (rc == MC_OK) rc = ok(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+                if (rep > 0 && ms < t_min) t_min = ms;
+            }
+            if (rc == MC_OK && t_min < best[which]) {
+                best[which] = t_min;
+                pick[which] = g;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    TRY(rc);
+    for (int q = 0; q < 3; ++q) CU(cudaMemcpyAsync(cur_n[q], save_n[q], bn, cudaMemcpyDeviceToDevice, s));
+    for (int q = 0; q < 2; ++q) CU(cudaMemcpyAsync(cur_m[q], save_m[q], bm, cudaMemcpyDeviceToDevice, s));
+    eng.g_col = pick[0];
+    eng.g_row = pick[1];
+    ctx.lane_cache[key] = {pick[0], pick[1]};
+    return MC_OK;
+}
 
 // Tiles of `per_tile` lines that never cross an LP boundary.
 static void make_tiles(const std::vector<long long>& off, int per_tile, std::vector<int>& lp, std::vector<int>& l0,
@@ -94,8 +263,7 @@ int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o,
     const double t_begin = now_ms();
     if (!lps || count <= 0 || !results) return set_error(MC_ERR_INVALID_ARGUMENT, "empty batch");
     TRY(validate_options(o));
-    if (o->precision != MC_PRECISION_FP64)
-        return set_error(MC_ERR_INVALID_ARGUMENT, "batched solves run the FP64 form");
+    const bool mixed = o->precision == MC_PRECISION_FP32_REFINE;
     if (o->lanes_per_column == -1 || o->lanes_per_row == -1)
         return set_error(MC_ERR_INVALID_ARGUMENT, "batched solves use the lane kernels");
     std::vector<long long> col_off(count + 1, 0), row_off(count + 1, 0), nnz_off(count + 1, 0);
@@ -143,6 +311,21 @@ int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o,
     const size_t o_st = L.add<DevState>(count + 1);
     const size_t o_off = L.add<double>(2LL * count);
     const size_t o_flags = L.add<int>(count);
+    const size_t o_active = L.add<int>(2LL * kMaxTiles + 2);
+    const bool tune = o->lanes_per_column == 0 || o->lanes_per_row == 0;
+    size_t o_save_n[3] = {0, 0, 0}, o_save_m[2] = {0, 0};
+    if (tune) {
+        for (auto& v : o_save_n) v = L.add<double>(n);
+        for (auto& v : o_save_m) v = L.add<double>(m);
+    }
+    // mixed form: FP32 matrix copies, FP32 correction iterates and cycle data
+    size_t o_f_cscv = 0, o_f_csrv = 0, o_fn[8] = {}, o_fm[7] = {};
+    if (mixed) {
+        o_f_cscv = L.add<float>(nnz + 16);
+        o_f_csrv = L.add<float>(nnz + 16);
+        for (auto& v : o_fn) v = L.add<float>(n);
+        for (auto& v : o_fm) v = L.add<float>(m);
+    }
     // iterates: x, x_bar, x_avg, dx (columns); y, y_avg, ax_bar (rows)
     size_t o_it_n[4], o_it_m[3];
     for (auto& v : o_it_n) v = L.add<double>(n);
@@ -255,6 +438,9 @@ int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o,
     B.offset = offsets;
     B.flags = flags;
     B.nlp = count;
+    int* active = static_cast<int*>(at(o_active));
+    B.active = active;
+    B.active_count = active + 2LL * kMaxTiles;
     int* tp = tiles;
     B.cols.lp = tp; tp += nct;
     B.cols.l0 = tp; tp += nct;
@@ -340,27 +526,125 @@ int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o,
     ctx.end_launch();
     TRY(ctx.launch_check("batch setup"));
 
-    EngineBatch eng;
-    eng.P = P;
-    eng.O = O;
-    eng.B = B;
-    eng.global = st + count;
-    eng.g_col = gc;
-    eng.g_row = gr;
     Controls ctl{o->primal_tolerance, o->dual_tolerance, o->gap_tolerance, o->restart_reduction_factor,
                  o->primal_weight_smoothing, o->restart_every, o->restart_strategy, o->adaptive_step_size,
                  o->adaptive_primal_weight};
     TraceBuf tr{0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-    ctx.begin_launch(MC_KERNEL_OTHER);
-    kb_all_done<<<1, 256, 0, s>>>(st, count, eng.global);
-    ctx.end_launch();
     const int poll_every = o->check_every_chunks > 0 ? o->check_every_chunks : 1;
-    TRY(run_chunks(ctx, eng, eng.global, o->max_iterations, o->restart_every, poll_every, ctl, tr));
+    auto setup_common = [&](BatchCommon& e) {
+        e.B = B;
+        e.global = st + count;
+        e.g_col = gc;
+        e.g_row = gr;
+        e.active = active;
+        e.active_count = active + 2LL * kMaxTiles;
+    };
+    // lanes: the autotuner where the options leave them open, else as given
+    auto tune_if_asked = [&](auto& e) -> int {
+        if (!tune) return MC_OK;
+        void* save_n[3];
+        void* save_m[2];
+        for (int q = 0; q < 3; ++q) save_n[q] = at(o_save_n[q]);
+        for (int q = 0; q < 2; ++q) save_m[q] = at(o_save_m[q]);
+        const int keep_col = e.g_col, keep_row = e.g_row;
+        TRY(tune_lanes(ctx, e, o->precision, save_n, save_m));
+        if (valid_lanes(o->lanes_per_column)) e.g_col = keep_col;
+        if (valid_lanes(o->lanes_per_row)) e.g_row = keep_row;
+        return MC_OK;
+    };
+    float* f_xa = nullptr;
+    float* f_ya = nullptr;
+    if (!mixed) {
+        EngineBatch eng;
+        setup_common(eng);
+        eng.P = P;
+        eng.O = O;
+        TRY(eng.compact(ctx));
+        TRY(tune_if_asked(eng));
+        TRY(run_chunks(ctx, eng, eng.global, o->max_iterations, o->restart_every, poll_every, ctl, tr));
+    } else {
+        EngineBatchMixed eng;
+        setup_common(eng);
+        float* f_cscv = static_cast<float*>(at(o_f_cscv));
+        float* f_csrv = static_cast<float*>(at(o_f_csrv));
+        float* fn[8];
+        float* fm[7];
+        for (int q = 0; q < 8; ++q) fn[q] = static_cast<float*>(at(o_fn[q]));
+        for (int q = 0; q < 7; ++q) fm[q] = static_cast<float*>(at(o_fm[q]));
+        const int nbz = blocks_for(ctx, nnz + 16, kBlock) * 4;
+        ctx.begin_launch(MC_KERNEL_SETUP);
+        k_to_float<<<nbz, kBlock, 0, s>>>(nnz + 16, cv, f_cscv);
+        ctx.end_launch();
+        ctx.begin_launch(MC_KERNEL_SETUP);
+        k_to_float<<<nbz, kBlock, 0, s>>>(nnz + 16, rv, f_csrv);
+        ctx.end_launch();
+        ctx.begin_launch(MC_KERNEL_SETUP);
+        k_to_float<<<blocks_for(ctx, n, kBlock), kBlock, 0, s>>>(n, col_norm, fn[3]);
+        ctx.end_launch();
+        ctx.begin_launch(MC_KERNEL_SETUP);
+        k_to_float<<<blocks_for(ctx, m, kBlock), kBlock, 0, s>>>(m, row_norm, fm[0]);
+        ctx.end_launch();
+        Iterates<float>& F = eng.P;
+        F.m = (int)m;
+        F.n = (int)n;
+        F.csc_start = cs;
+        F.csc_row = ri;
+        F.csc_val = f_cscv;
+        F.csr_start = rs;
+        F.csr_col = ci;
+        F.csr_val = f_csrv;
+        F.c = fn[0];
+        F.lo = fn[1];
+        F.hi = fn[2];
+        F.blo = nullptr;  // the mixed dual step reads r_lo / r_hi instead
+        F.bhi = nullptr;
+        F.col_norm = fn[3];
+        F.row_norm = fm[0];
+        F.x = fn[4];
+        F.x_bar = fn[5];
+        F.x_avg = fn[6];
+        F.dx = fn[7];
+        F.y = fm[1];
+        F.y_avg = fm[2];
+        F.ax_bar = fm[3];
+        F.partials = partials;
+        F.st = st;
+        MixedState& M = eng.M;
+        M.x_hat = P.x;  // every LP's FP64 start point is its first base
+        M.y_hat = P.y;
+        M.ax_full = P.ax_bar;
+        M.aty_full = P.dx;
+        M.c64 = c;
+        M.lo64 = lo;
+        M.hi64 = hi;
+        M.blo64 = blo;
+        M.bhi64 = bhi;
+        M.csc_val64 = cv;
+        M.csr_val64 = rv;
+        M.g = fn[0];
+        M.lo = fn[1];
+        M.hi = fn[2];
+        M.r_lo = fm[4];
+        M.r_hi = fm[5];
+        M.yb = fm[6];
+        eng.O = O;
+        f_xa = F.x_avg;
+        f_ya = F.y_avg;
+        for (int q = 4; q < 8; ++q) CU(cudaMemsetAsync(fn[q], 0, sizeof(float) * (size_t)n, s));
+        for (int q = 1; q < 4; ++q) CU(cudaMemsetAsync(fm[q], 0, sizeof(float) * (size_t)m, s));
+        TRY(eng.compact(ctx));
+        // the first correction LP of every running LP, around its start point
+        TRY(eng.residual_pass(ctx));
+        TRY(eng.recenter(ctx, 1));
+        TRY(tune_if_asked(eng));
+        TRY(run_chunks(ctx, eng, eng.global, o->max_iterations, o->restart_every, poll_every, ctl, tr));
+    }
     CU(cudaEventRecord(ctx.ev_c, s));
 
     // ---- outputs
     ctx.begin_launch(MC_KERNEL_OTHER);
-    kb_unscale_out<<<nct + nrt, kBlock, 0, s>>>(P, col_scale, row_scale, stage_x, stage_y, B);
+    kb_unscale_out<<<nct + nrt, kBlock, 0, s>>>(mixed ? P.x : P.x_avg, f_xa, mixed ? P.y : P.y_avg, f_ya, col_scale,
+                                                row_scale, stage_x, stage_y, B);
     ctx.end_launch();
     TRY(ctx.launch_check("batch unscale"));
     for (int b = 0; b < count; ++b) {
@@ -410,6 +694,8 @@ int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o,
         r.final_primal_weight = S.omega;
         r.final_step_size = S.eta;
         r.kernel_launches = total;
+        r.refinement_rounds = mixed ? S.restarts : 0;  // each restart re-centres the LP's FP64 base
+        r.inner_iterations = mixed ? S.iter : 0;
         for (int q = 0; q < MC_KERNEL_KINDS; ++q) {
             r.launches_by_kind[q] = ctx.launches[q];
             r.kernel_ms_by_kind[q] = ctx.kernel_ms[q];

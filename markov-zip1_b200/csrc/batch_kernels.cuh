@@ -1,16 +1,22 @@
 // Batched PDLP: many independent LPs of uneven size solved together.
 //
 // The LPs are packed block-diagonally into one CSC and one CSR (column block
-// b holds LP b's columns, row block b its rows).  Every kernel launches one
-// block per tile; a tile is a run of consecutive lines (columns or rows) of
-// ONE LP, so a block reads that LP's scalars once (its DevState: eta, omega,
-// averaging count, restart and termination state) and writes its reduction
-// partial to its own slot.  The per-LP reductions then read the LP's tile
-// range in order: every LP follows the reference algorithm
+// b holds LP b's columns, row block b its rows).  A tile is a run of
+// consecutive lines (columns or rows) of ONE LP, so a block working on it
+// reads that LP's scalars once (its DevState: eta, omega, averaging count,
+// restart and termination state) and writes the tile's reduction partial to
+// the tile's own slot.  The per-LP reductions then read the LP's tile range in
+// order: every LP follows the reference algorithm
 // (src/lp/first_order/pdlp.cpp:139-276) on its own -- own step size, own
 // primal weight, own restarts and termination -- exactly as if it were solved
-// alone, and the results are run-to-run deterministic.  All LPs advance in
-// lockstep; an LP that has terminated costs one flag read per tile.
+// alone, and the results are run-to-run deterministic.
+//
+// Work queue: the iteration kernels are persistent (one wave of resident
+// blocks) and walk a compacted list of the tiles whose LP is still running,
+// block b taking entries b, b + grid, b + 2 grid, ...  kb_compact rebuilds the
+// list after every restart check (the only place an LP terminates), so an LP
+// that has converged costs nothing from its next chunk on, and the long tail
+// where a few slow LPs run on alone costs only their own tiles.
 //
 // The row and column work inside a tile is the single-LP kernels' (lanes per
 // line, cache policies, fused updates), so the per-nonzero cost is the same.
@@ -18,6 +24,7 @@
 
 #include "common.cuh"
 #include "iter_kernels.cuh"
+#include "mixed.cuh"
 #include "setup_kernels.cuh"
 
 namespace mc {
@@ -30,108 +37,111 @@ struct TileTable {
     int ntiles;
 };
 
+constexpr int kMaxTiles = 1 << 17;  // per-slot capacity of the batch partials buffer
+
 struct BatchRefs {
     DevState* st;              // [nlp]
     const double* offset;      // [nlp] objective offsets
     int* flags;                // [nlp] setup certificates: 1 crossed bounds, 2 row activity
     TileTable cols, rows;
+    const int* active;         // [2 * kMaxTiles] running column tiles, then running row tiles
+    const int* active_count;   // [2] lengths of the two lists
     int nlp;
 };
 
-constexpr int kMaxTiles = 1 << 17;  // per-slot capacity of the batch partials buffer
+// The running tiles of one kind (0 columns, 1 rows), grid-strided over the
+// persistent blocks; T is the tile's index in its table.
+#define MC_FOR_ACTIVE(B, WHICH, T)                                                                  \
+    for (int q_ = blockIdx.x, nq_ = B.active_count[WHICH]; q_ < nq_; q_ += gridDim.x)             \
+        if (const int T = B.active[(WHICH) * kMaxTiles + q_]; true)
 
-// Lines of this block's tile, G lanes per line; every thread of the block
-// makes the same number of trips (the shuffles need all lanes).
-#define MC_TILE_LINES(TT, LINE, VALID, SUB)                                                          \
+// Lines of tile T, G lanes per line; every thread of the block makes the same
+// number of trips (the shuffles need all lanes).
+#define MC_TILE_LINES(TT, T, LINE, VALID, SUB)                                                       \
     const int SUB = threadIdx.x % G;                                                                \
-    const int tl1_ = TT.l1[blockIdx.x];                                                             \
-    for (int base_ = TT.l0[blockIdx.x], LINE = 0;                                                   \
+    const int tl1_ = TT.l1[T];                                                                      \
+    for (int base_ = TT.l0[T], LINE = 0;                                                            \
          base_ < tl1_ && ((LINE = base_ + (int)(threadIdx.x / G)), true); base_ += kBlock / G)     \
         if (const bool VALID = LINE < tl1_; true)
 
 // ------------------------------------------------------------------ primal
-template <int G, bool STEP>
-__global__ void __launch_bounds__(kBlock) kb_primal(Iterates<double> P, BatchRefs B, int k) {
+template <int G, bool STEP, class T>
+__global__ void __launch_bounds__(kBlock) kb_primal(Iterates<T> P, BatchRefs B, int k) {
     __shared__ double scratch[32];
-    const int lp = B.cols.lp[blockIdx.x];
-    const DevState* st = B.st + lp;
-    if (st->done) {
-        if (STEP && threadIdx.x == 0) P.partials[SLOT_DX * kMaxTiles + blockIdx.x] = 0.0;
-        return;
-    }
-    const double step = st->eta / st->omega;
-    const double cnt = (double)(st->avg_count + k + 1);
     const unsigned long long pol = policy_keep();
-    double acc = 0.0;
-    MC_TILE_LINES(B.cols, j, valid, sub) {
-        const bool owner = valid && sub == 0;
-        double cn = 1.0, cj = 0.0, xo = 0.0, lj = 0.0, hj = 0.0, xa = 0.0;
-        if (owner) {
-            cn = ld_stream(P.col_norm + j);
-            cj = ld_stream(P.c + j);
-            xo = ld_stream(P.x + j);
-            lj = ld_stream(P.lo + j);
-            hj = ld_stream(P.hi + j);
-            xa = ld_stream(P.x_avg + j);
-        }
-        const double aty = line_dot<G>(P.csc_start, P.csc_row, P.csc_val, P.y, j, valid, sub, pol);
-        if (owner) {
-            const double g = __dadd_rn(cj, aty);
-            const double tau = __ddiv_rn(step, cn);
-            const double xp = clampv(__dsub_rn(xo, __dmul_rn(tau, g)), lj, hj);
-            const double d = __dsub_rn(xp, xo);
-            if (STEP) {
-                st_keep(P.dx + j, d, pol);
-                acc += __dmul_rn(__dmul_rn(cn, d), d);
+    MC_FOR_ACTIVE(B, 0, t) {
+        const DevState* st = B.st + B.cols.lp[t];
+        const T step = T(st->eta / st->omega);
+        const T cnt = T((double)(st->avg_count + k + 1));
+        double acc = 0.0;
+        MC_TILE_LINES(B.cols, t, j, valid, sub) {
+            const bool owner = valid && sub == 0;
+            T cn = T(1), cj = T(0), xo = T(0), lj = T(0), hj = T(0), xa = T(0);
+            if (owner) {
+                cn = ld_stream(P.col_norm + j);
+                cj = ld_stream(P.c + j);
+                xo = ld_stream(P.x + j);
+                lj = ld_stream(P.lo + j);
+                hj = ld_stream(P.hi + j);
+                xa = ld_stream(P.x_avg + j);
             }
-            st_stream(P.x + j, xp);
-            st_keep(P.x_bar + j, __dsub_rn(__dmul_rn(2.0, xp), xo), pol);
-            st_stream(P.x_avg + j, __dadd_rn(xa, __ddiv_rn(__dsub_rn(xp, xa), cnt)));
+            const T aty = line_dot<G>(P.csc_start, P.csc_row, P.csc_val, P.y, j, valid, sub, pol);
+            if (owner) {
+                const T g = add_rn(cj, aty);
+                const T tau = div_rn(step, cn);
+                const T xp = clampv(sub_rn(xo, mul_rn(tau, g)), lj, hj);
+                const T d = sub_rn(xp, xo);
+                if (STEP) {
+                    st_keep(P.dx + j, d, pol);
+                    acc += __dmul_rn(__dmul_rn((double)cn, (double)d), (double)d);
+                }
+                st_stream(P.x + j, xp);
+                st_keep(P.x_bar + j, sub_rn(mul_rn(T(2), xp), xo), pol);
+                st_stream(P.x_avg + j, add_rn(xa, div_rn(sub_rn(xp, xa), cnt)));
+            }
         }
-    }
-    if (STEP) {
-        acc = block_reduce(acc, scratch, OpSum());
-        if (threadIdx.x == 0) P.partials[SLOT_DX * kMaxTiles + blockIdx.x] = acc;
+        if (STEP) {
+            acc = block_reduce(acc, scratch, OpSum());
+            if (threadIdx.x == 0) P.partials[SLOT_DX * kMaxTiles + t] = acc;
+        }
     }
 }
 
 // -------------------------------------------------------------------- dual
 template <int G>
 __global__ void __launch_bounds__(kBlock) kb_dual(Iterates<double> P, BatchRefs B, int k) {
-    const int lp = B.rows.lp[blockIdx.x];
-    const DevState* st = B.st + lp;
-    if (st->done) return;
-    const double sg = st->eta * st->omega;
-    const double cnt = (double)(st->avg_count + k + 1);
     const unsigned long long pol = policy_keep();
-    MC_TILE_LINES(B.rows, i, valid, sub) {
-        RowData<double> r{};
-        if (valid && sub == 0) r = load_row(P, i);
-        const double ax = line_dot<G>(P.csr_start, P.csr_col, P.csr_val, P.x_bar, i, valid, sub, pol);
-        if (valid && sub == 0) dual_update(P, i, r, ax, sg, cnt, pol);
+    MC_FOR_ACTIVE(B, 1, t) {
+        const DevState* st = B.st + B.rows.lp[t];
+        const double sg = st->eta * st->omega;
+        const double cnt = (double)(st->avg_count + k + 1);
+        MC_TILE_LINES(B.rows, t, i, valid, sub) {
+            RowData<double> r{};
+            if (valid && sub == 0) r = load_row(P, i);
+            const double ax = line_dot<G>(P.csr_start, P.csr_col, P.csr_val, P.x_bar, i, valid, sub, pol);
+            if (valid && sub == 0) dual_update(P, i, r, ax, sg, cnt, pol);
+        }
     }
 }
 
-template <int G>
-__global__ void __launch_bounds__(kBlock) kb_dual_probe(Iterates<double> P, BatchRefs B) {
+template <int G, class T>
+__global__ void __launch_bounds__(kBlock) kb_dual_probe(Iterates<T> P, BatchRefs B) {
     __shared__ double scratch[32];
-    const int lp = B.rows.lp[blockIdx.x];
-    if (B.st[lp].done) {
-        if (threadIdx.x == 0) P.partials[SLOT_ADX * kMaxTiles + blockIdx.x] = 0.0;
-        return;
-    }
     const unsigned long long pol = policy_keep();
-    double acc = 0.0;
-    MC_TILE_LINES(B.rows, i, valid, sub) {
-        double axb, adx;
-        line_dot2<G>(P.csr_start, P.csr_col, P.csr_val, P.x_bar, P.dx, i, valid, sub, axb, adx, pol);
-        if (valid && sub == 0) {
-            P.ax_bar[i] = axb;
-            acc += __ddiv_rn(__dmul_rn(adx, adx), P.row_norm[i]);
+    MC_FOR_ACTIVE(B, 1, t) {
+        double acc = 0.0;
+        MC_TILE_LINES(B.rows, t, i, valid, sub) {
+            T axb, adx;
+            line_dot2<G>(P.csr_start, P.csr_col, P.csr_val, P.x_bar, P.dx, i, valid, sub, axb, adx, pol);
+            if (valid && sub == 0) {
+                P.ax_bar[i] = axb;
+                const double a = (double)adx;
+                acc += __ddiv_rn(__dmul_rn(a, a), (double)P.row_norm[i]);
+            }
         }
+        acc = block_reduce(acc, scratch, OpSum());
+        if (threadIdx.x == 0) P.partials[SLOT_ADX * kMaxTiles + t] = acc;
     }
-    acc = block_reduce(acc, scratch, OpSum());
-    if (threadIdx.x == 0) P.partials[SLOT_ADX * kMaxTiles + blockIdx.x] = acc;
 }
 
 // one block per LP: the adaptive eta rule (pdlp.cpp:207-219) on the LP's sums
@@ -156,24 +166,23 @@ __global__ void kb_step_size(const double* __restrict__ partials, BatchRefs B, C
 }
 
 __global__ void __launch_bounds__(kBlock) kb_dual_apply(Iterates<double> P, BatchRefs B, int k) {
-    const int lp = B.rows.lp[blockIdx.x];
-    const DevState* st = B.st + lp;
-    if (st->done) return;
-    const double sg = st->eta * st->omega;
-    const double cnt = (double)(st->avg_count + k + 1);
     const unsigned long long pol = policy_keep();
-    for (int i = B.rows.l0[blockIdx.x] + threadIdx.x; i < B.rows.l1[blockIdx.x]; i += blockDim.x)
-        dual_update(P, i, P.ax_bar[i], sg, cnt, pol);
+    MC_FOR_ACTIVE(B, 1, t) {
+        const DevState* st = B.st + B.rows.lp[t];
+        const double sg = st->eta * st->omega;
+        const double cnt = (double)(st->avg_count + k + 1);
+        for (int i = B.rows.l0[t] + threadIdx.x; i < B.rows.l1[t]; i += blockDim.x)
+            dual_update(P, i, P.ax_bar[i], sg, cnt, pol);
+    }
 }
 
 // --------------------------------------------------------------- residuals
 template <int G>
 __global__ void __launch_bounds__(kBlock) kb_residual_rows(Iterates<double> P, Original O, BatchRefs B) {
     __shared__ double scratch[32];
-    const int lp = B.rows.lp[blockIdx.x];
-    RowTerms acc;
-    if (!B.st[lp].done) {
-        MC_TILE_LINES(B.rows, i, valid, sub) {
+    MC_FOR_ACTIVE(B, 1, t) {
+        RowTerms acc;
+        MC_TILE_LINES(B.rows, t, i, valid, sub) {
             double s = 0.0;
             if (valid) {
                 const int b = P.csr_start[i], e = P.csr_start[i + 1];
@@ -182,24 +191,23 @@ __global__ void __launch_bounds__(kBlock) kb_residual_rows(Iterates<double> P, O
             s = group_sum<G>(s);
             if (valid && sub == 0) acc.add(O, i, s, P.y_avg[i]);
         }
-    }
-    acc.vmax = block_reduce(acc.vmax, scratch, OpMax());
-    acc.dsum = block_reduce(acc.dsum, scratch, OpSum());
-    acc.bad = block_reduce(acc.bad, scratch, OpSum());
-    if (threadIdx.x == 0) {
-        P.partials[SLOT_ROW_MAX * kMaxTiles + blockIdx.x] = acc.vmax;
-        P.partials[SLOT_ROW_DOBJ * kMaxTiles + blockIdx.x] = acc.dsum;
-        P.partials[SLOT_NAN * kMaxTiles + blockIdx.x] = acc.bad;
+        acc.vmax = block_reduce(acc.vmax, scratch, OpMax());
+        acc.dsum = block_reduce(acc.dsum, scratch, OpSum());
+        acc.bad = block_reduce(acc.bad, scratch, OpSum());
+        if (threadIdx.x == 0) {
+            P.partials[SLOT_ROW_MAX * kMaxTiles + t] = acc.vmax;
+            P.partials[SLOT_ROW_DOBJ * kMaxTiles + t] = acc.dsum;
+            P.partials[SLOT_NAN * kMaxTiles + t] = acc.bad;
+        }
     }
 }
 
 template <int G>
 __global__ void __launch_bounds__(kBlock) kb_residual_cols(Iterates<double> P, Original O, BatchRefs B) {
     __shared__ double scratch[32];
-    const int lp = B.cols.lp[blockIdx.x];
-    ColTerms acc;
-    if (!B.st[lp].done) {
-        MC_TILE_LINES(B.cols, j, valid, sub) {
+    MC_FOR_ACTIVE(B, 0, t) {
+        ColTerms acc;
+        MC_TILE_LINES(B.cols, t, j, valid, sub) {
             double s = 0.0;
             if (valid) {
                 const int b = P.csc_start[j], e = P.csc_start[j + 1];
@@ -208,18 +216,18 @@ __global__ void __launch_bounds__(kBlock) kb_residual_cols(Iterates<double> P, O
             s = group_sum<G>(s);
             if (valid && sub == 0) acc.add(O, j, s, P.x_avg[j]);
         }
-    }
-    acc.vmax = block_reduce(acc.vmax, scratch, OpMax());
-    acc.dres = block_reduce(acc.dres, scratch, OpSum());
-    acc.pobj = block_reduce(acc.pobj, scratch, OpSum());
-    acc.dobj = block_reduce(acc.dobj, scratch, OpSum());
-    acc.bad = block_reduce(acc.bad, scratch, OpSum());
-    if (threadIdx.x == 0) {
-        P.partials[SLOT_COL_MAX * kMaxTiles + blockIdx.x] = acc.vmax;
-        P.partials[SLOT_COL_DRES * kMaxTiles + blockIdx.x] = acc.dres;
-        P.partials[SLOT_COL_POBJ * kMaxTiles + blockIdx.x] = acc.pobj;
-        P.partials[SLOT_COL_DOBJ * kMaxTiles + blockIdx.x] = acc.dobj;
-        P.partials[SLOT_B * kMaxTiles + blockIdx.x] = acc.bad;
+        acc.vmax = block_reduce(acc.vmax, scratch, OpMax());
+        acc.dres = block_reduce(acc.dres, scratch, OpSum());
+        acc.pobj = block_reduce(acc.pobj, scratch, OpSum());
+        acc.dobj = block_reduce(acc.dobj, scratch, OpSum());
+        acc.bad = block_reduce(acc.bad, scratch, OpSum());
+        if (threadIdx.x == 0) {
+            P.partials[SLOT_COL_MAX * kMaxTiles + t] = acc.vmax;
+            P.partials[SLOT_COL_DRES * kMaxTiles + t] = acc.dres;
+            P.partials[SLOT_COL_POBJ * kMaxTiles + t] = acc.pobj;
+            P.partials[SLOT_COL_DOBJ * kMaxTiles + t] = acc.dobj;
+            P.partials[SLOT_B * kMaxTiles + t] = acc.bad;
+        }
     }
 }
 
@@ -288,16 +296,19 @@ __global__ void kb_finalize(const double* __restrict__ partials, BatchRefs B, lo
     if (!final_pass) st->checks += 1;
 }
 
-// restart to the average, per tile (columns tiles then row tiles)
+// restart to the average, over the running tiles (columns, then rows)
 __global__ void __launch_bounds__(kBlock) kb_restart_copy(Iterates<double> P, BatchRefs B) {
-    const bool col = blockIdx.x < (unsigned)B.cols.ntiles;
-    const int t = col ? blockIdx.x : blockIdx.x - B.cols.ntiles;
-    const TileTable& T = col ? B.cols : B.rows;
-    const DevState* st = B.st + T.lp[t];
-    if (!st->restart_pending || st->done) return;
-    for (int l = T.l0[t] + threadIdx.x; l < T.l1[t]; l += blockDim.x) {
-        if (col) P.x[l] = P.x_avg[l];
-        else P.y[l] = P.y_avg[l];
+    const int nc = B.active_count[0], nr = B.active_count[1];
+    for (int q = blockIdx.x; q < nc + nr; q += gridDim.x) {
+        const bool col = q < nc;
+        const int t = col ? B.active[q] : B.active[kMaxTiles + q - nc];
+        const TileTable& T = col ? B.cols : B.rows;
+        const DevState* st = B.st + T.lp[t];
+        if (!st->restart_pending || st->done) continue;
+        for (int l = T.l0[t] + threadIdx.x; l < T.l1[t]; l += blockDim.x) {
+            if (col) P.x[l] = P.x_avg[l];
+            else P.y[l] = P.y_avg[l];
+        }
     }
 }
 
@@ -494,16 +505,19 @@ __global__ void kb_setup_scalars(const double* __restrict__ partials, BatchRefs 
     }
 }
 
-// per-tile unscaled output (k_unscale_out over the tile's lines)
-__global__ void kb_unscale_out(Iterates<double> P, const double* __restrict__ col_scale,
-                               const double* __restrict__ row_scale, double* __restrict__ x_out,
-                               double* __restrict__ y_out, BatchRefs B) {
+// per-tile unscaled output (k_unscale_out over the tile's lines): x = x_avg
+// D_C, y = y_avg D_R; in the mixed form the averages are the FP64 base plus
+// the FP32 average correction (dx_avg, dy_avg non-null)
+__global__ void kb_unscale_out(const double* __restrict__ x_avg, const float* __restrict__ dx_avg,
+                               const double* __restrict__ y_avg, const float* __restrict__ dy_avg,
+                               const double* __restrict__ col_scale, const double* __restrict__ row_scale,
+                               double* __restrict__ x_out, double* __restrict__ y_out, BatchRefs B) {
     const bool col = blockIdx.x < (unsigned)B.cols.ntiles;
     const int t = col ? blockIdx.x : blockIdx.x - B.cols.ntiles;
     const TileTable& T = col ? B.cols : B.rows;
     for (int l = T.l0[t] + threadIdx.x; l < T.l1[t]; l += blockDim.x) {
-        if (col) x_out[l] = __dmul_rn(P.x_avg[l], col_scale[l]);
-        else y_out[l] = __dmul_rn(P.y_avg[l], row_scale[l]);
+        if (col) x_out[l] = __dmul_rn(dx_avg ? x_avg[l] + (double)dx_avg[l] : x_avg[l], col_scale[l]);
+        else y_out[l] = __dmul_rn(dy_avg ? y_avg[l] + (double)dy_avg[l] : y_avg[l], row_scale[l]);
     }
 }
 
@@ -517,18 +531,208 @@ __global__ void kb_shift_indices(int* __restrict__ col_start, int* __restrict__ 
     }
 }
 
-// the packed loop's poll flag: done once every LP is done
-__global__ void kb_all_done(const DevState* __restrict__ st, int nlp, DevState* __restrict__ global) {
+// The work queue (one block of kCompactThreads): the running column and row
+// tiles in table order, and the packed loop's poll flag (done once every LP is
+// done).  An ordered compaction: ballots give each warp's survivors, a scan
+// of the warp totals their offsets.
+constexpr int kCompactThreads = 1024;
+
+__global__ void __launch_bounds__(kCompactThreads) kb_compact(BatchRefs B, int* __restrict__ active,
+                                                              int* __restrict__ active_count,
+                                                              DevState* __restrict__ global) {
+    __shared__ int warp_total[32];
+    __shared__ int base;
     __shared__ int running;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int kWarps = kCompactThreads / 32;
+    for (int which = 0; which < 2; ++which) {
+        const TileTable& T = which ? B.rows : B.cols;
+        int* out = active + which * kMaxTiles;
+        if (threadIdx.x == 0) base = 0;
+        __syncthreads();
+        for (int t0 = 0; t0 < T.ntiles; t0 += kCompactThreads) {
+            const int t = t0 + threadIdx.x;
+            const bool keep = t < T.ntiles && !B.st[T.lp[t]].done;
+            const unsigned ballot = __ballot_sync(0xffffffffu, keep);
+            if (lane == 0) warp_total[warp] = __popc(ballot);
+            __syncthreads();
+            if (warp == 0) {
+                int v = warp_total[lane];
+#pragma unroll
+                for (int off = 1; off < 32; off <<= 1) {
+                    const int u = __shfl_up_sync(0xffffffffu, v, off);
+                    if (lane >= off) v += u;
+                }
+                warp_total[lane] = v;  // inclusive prefix over warps
+            }
+            __syncthreads();
+            if (keep) out[base + (warp ? warp_total[warp - 1] : 0) + __popc(ballot & ((1u << lane) - 1u))] = t;
+            __syncthreads();
+            if (threadIdx.x == 0) base += warp_total[kWarps - 1];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) active_count[which] = base;
+        __syncthreads();
+    }
     if (threadIdx.x == 0) running = 0;
     __syncthreads();
     int c = 0;
-    for (int b = threadIdx.x; b < nlp; b += blockDim.x) c += st[b].done ? 0 : 1;
+    for (int b = threadIdx.x; b < B.nlp; b += blockDim.x) c += B.st[b].done ? 0 : 1;
     if (c) atomicAdd(&running, c);
     __syncthreads();
     if (threadIdx.x == 0) global->done = running == 0 ? 1 : 0;
 }
 
+// ------------------------------------------------- mixed precision, batched
+// The FP32 + FP64-refinement form (mixed.cuh) per LP: the correction LP of
+// every LP is iterated in FP32 over the packed FP32 matrix, its residuals,
+// restart and termination are evaluated in FP64, and at each restart of an LP
+// its base moves to the average and its correction data are rebuilt.
+
+template <int G>
+__global__ void __launch_bounds__(kBlock) kb_dual_mx(Iterates<float> P, MixedState M, BatchRefs B, int k) {
+    const unsigned long long pol = policy_keep();
+    MC_FOR_ACTIVE(B, 1, t) {
+        const DevState* st = B.st + B.rows.lp[t];
+        const float sg = (float)(st->eta * st->omega);
+        const float cnt = (float)(double)(st->avg_count + k + 1);
+        MC_TILE_LINES(B.rows, t, i, valid, sub) {
+            const bool owner = valid && sub == 0;
+            float rn = 1.f, dy = 0.f, dya = 0.f, yb = 0.f, rl = 0.f, rh = 0.f;
+            if (owner) {
+                rn = ld_stream(P.row_norm + i);
+                dy = ld_stream(P.y + i);
+                dya = ld_stream(P.y_avg + i);
+                yb = ld_stream(M.yb + i);
+                rl = ld_stream(M.r_lo + i);
+                rh = ld_stream(M.r_hi + i);
+            }
+            const float ax = line_dot<G>(P.csr_start, P.csr_col, P.csr_val, P.x_bar, i, valid, sub, pol);
+            if (owner) dual_update_mx(P, M, i, ax, sg, cnt, pol, rn, dy, dya, yb, rl, rh);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) kb_dual_apply_mx(Iterates<float> P, MixedState M, BatchRefs B, int k) {
+    const unsigned long long pol = policy_keep();
+    MC_FOR_ACTIVE(B, 1, t) {
+        const DevState* st = B.st + B.rows.lp[t];
+        const float sg = (float)(st->eta * st->omega);
+        const float cnt = (float)(double)(st->avg_count + k + 1);
+        for (int i = B.rows.l0[t] + threadIdx.x; i < B.rows.l1[t]; i += blockDim.x)
+            dual_update_mx(P, M, i, P.ax_bar[i], sg, cnt, pol, ld_stream(P.row_norm + i), ld_stream(P.y + i),
+                           ld_stream(P.y_avg + i), ld_stream(M.yb + i), ld_stream(M.r_lo + i),
+                           ld_stream(M.r_hi + i));
+    }
+}
+
+// FP64 residual pass of each running LP on x_hat + dx_avg, y_hat + dy_avg,
+// keeping A x and A^T y of that point for the recentring.
+template <int G>
+__global__ void __launch_bounds__(kBlock) kb_residual_rows_mx(Iterates<float> P, MixedState M, Original O,
+                                                              BatchRefs B) {
+    __shared__ double scratch[32];
+    MC_FOR_ACTIVE(B, 1, t) {
+        RowTerms acc;
+        MC_TILE_LINES(B.rows, t, i, valid, sub) {
+            double s = 0.0;
+            if (valid) {
+                const int b = P.csr_start[i], e = P.csr_start[i + 1];
+                for (int p = b + sub; p < e; p += G) {
+                    const int jj = P.csr_col[p];
+                    s = fma(M.csr_val64[p], M.x_hat[jj] + (double)P.x_avg[jj], s);
+                }
+            }
+            s = group_sum<G>(s);
+            if (valid && sub == 0) {
+                M.ax_full[i] = s;
+                acc.add(O, i, s, M.y_hat[i] + (double)P.y_avg[i]);
+            }
+        }
+        acc.vmax = block_reduce(acc.vmax, scratch, OpMax());
+        acc.dsum = block_reduce(acc.dsum, scratch, OpSum());
+        acc.bad = block_reduce(acc.bad, scratch, OpSum());
+        if (threadIdx.x == 0) {
+            P.partials[SLOT_ROW_MAX * kMaxTiles + t] = acc.vmax;
+            P.partials[SLOT_ROW_DOBJ * kMaxTiles + t] = acc.dsum;
+            P.partials[SLOT_NAN * kMaxTiles + t] = acc.bad;
+        }
+    }
+}
+
+template <int G>
+__global__ void __launch_bounds__(kBlock) kb_residual_cols_mx(Iterates<float> P, MixedState M, Original O,
+                                                              BatchRefs B) {
+    __shared__ double scratch[32];
+    MC_FOR_ACTIVE(B, 0, t) {
+        ColTerms acc;
+        MC_TILE_LINES(B.cols, t, j, valid, sub) {
+            double s = 0.0;
+            if (valid) {
+                const int b = P.csc_start[j], e = P.csc_start[j + 1];
+                for (int p = b + sub; p < e; p += G) {
+                    const int ii = P.csc_row[p];
+                    s = fma(M.csc_val64[p], M.y_hat[ii] + (double)P.y_avg[ii], s);
+                }
+            }
+            s = group_sum<G>(s);
+            if (valid && sub == 0) {
+                M.aty_full[j] = s;
+                acc.add(O, j, s, M.x_hat[j] + (double)P.x_avg[j]);
+            }
+        }
+        acc.vmax = block_reduce(acc.vmax, scratch, OpMax());
+        acc.dres = block_reduce(acc.dres, scratch, OpSum());
+        acc.pobj = block_reduce(acc.pobj, scratch, OpSum());
+        acc.dobj = block_reduce(acc.dobj, scratch, OpSum());
+        acc.bad = block_reduce(acc.bad, scratch, OpSum());
+        if (threadIdx.x == 0) {
+            P.partials[SLOT_COL_MAX * kMaxTiles + t] = acc.vmax;
+            P.partials[SLOT_COL_DRES * kMaxTiles + t] = acc.dres;
+            P.partials[SLOT_COL_POBJ * kMaxTiles + t] = acc.pobj;
+            P.partials[SLOT_COL_DOBJ * kMaxTiles + t] = acc.dobj;
+            P.partials[SLOT_B * kMaxTiles + t] = acc.bad;
+        }
+    }
+}
+
+// Restart of an LP to its average in the mixed form: its base moves there and
+// its correction LP's data are rebuilt from the residual pass's FP64 products
+// (k_recenter_mx per LP).  `force` rebuilds every running LP (the start).
+__global__ void __launch_bounds__(kBlock) kb_recenter_mx(Iterates<float> P, MixedState M, BatchRefs B, int force) {
+    const float inf = __int_as_float(0x7f800000);
+    const int nc = B.active_count[0], nr = B.active_count[1];
+    for (int q = blockIdx.x; q < nc + nr; q += gridDim.x) {
+        const bool col = q < nc;
+        const int t = col ? B.active[q] : B.active[kMaxTiles + q - nc];
+        const TileTable& T = col ? B.cols : B.rows;
+        const DevState* st = B.st + T.lp[t];
+        if (st->done || (!force && !st->restart_pending)) continue;
+        for (int l = T.l0[t] + threadIdx.x; l < T.l1[t]; l += blockDim.x) {
+            if (col) {
+                const double xh = M.x_hat[l] + (double)P.x_avg[l];
+                M.x_hat[l] = xh;
+                P.x[l] = 0.f;
+                P.x_avg[l] = 0.f;
+                M.g[l] = (float)(M.c64[l] + M.aty_full[l]);
+                const double lo = M.lo64[l], hi = M.hi64[l];
+                M.lo[l] = (lo <= -1e299) ? -inf : (float)(lo - xh);
+                M.hi[l] = (hi >= 1e299) ? inf : (float)(hi - xh);
+            } else {
+                const double yh = M.y_hat[l] + (double)P.y_avg[l];
+                M.y_hat[l] = yh;
+                P.y[l] = 0.f;
+                P.y_avg[l] = 0.f;
+                M.yb[l] = (float)yh;
+                const double ax = M.ax_full[l], lo = M.blo64[l], hi = M.bhi64[l];
+                M.r_lo[l] = (lo <= -1e299) ? inf : (float)(ax - lo);
+                M.r_hi[l] = (hi >= 1e299) ? -inf : (float)(ax - hi);
+            }
+        }
+    }
+}
+
 #undef MC_TILE_LINES
+#undef MC_FOR_ACTIVE
 
 }  // namespace mc

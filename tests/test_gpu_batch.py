@@ -89,3 +89,65 @@ def test_batch_iteration_limit_and_trivial_members(gpu_ctx):
     assert res[0].iterations == res[2].iterations == 55
     assert res[0].objective == res[2].objective
     assert res[1].status == PdlpStatus.optimal and res[1].message == "trivial"
+
+
+def test_mixed_batch_matches_solo_solves(gpu_ctx, oracle):
+    """FP32 + FP64-refinement batch: every LP still reaches 1e-8 relative KKT
+    (residuals evaluated in FP64) and agrees with the oracle's solo solve and
+    the analytic optimum within 1e-6."""
+    from mcpdlp import Precision
+    models = generators.batch_part1(7, count=8, m_range=(100, 600))
+    res = gpu_ctx.solve_batch(models, opts(1e-8, precision=Precision.fp32_refine))
+    for m, r in zip(models, res):
+        cpu = oracle.solve(m, options(1e-8))
+        assert r.status == cpu.status == PdlpStatus.optimal, m.name
+        assert max(r.primal_infeasibility, r.dual_infeasibility, r.duality_gap) <= 1e-8
+        assert rel(r.objective, cpu.objective) <= 1e-6, m.name
+        assert rel(r.objective, m.info["optimum"]) <= 1e-6, m.name
+        assert r.extra["refinement_rounds"] == r.extra["restarts"] > 0
+
+
+def test_mixed_batch_node_variants(gpu_ctx, oracle):
+    from mcpdlp import Precision
+    base, variants, _ = generators.batch_part2(3, variants=16, m=400, n=1200, k=8)
+    res = gpu_ctx.solve_batch(variants, opts(1e-6, precision=Precision.fp32_refine))
+    for v, r in zip(variants, res):
+        if np.any(v.var_lower > v.var_upper):
+            assert r.status == PdlpStatus.infeasible_or_unbounded, v.name
+            continue
+        cpu = oracle.solve(v, options(1e-6, max_iterations=20000))
+        if cpu.status == PdlpStatus.optimal:
+            assert r.status == PdlpStatus.optimal, v.name
+            assert rel(r.objective, cpu.objective) <= 1e-4, v.name
+
+
+@pytest.mark.parametrize("lanes", [(1, 1), (2, 8), (32, 32)])
+def test_batch_lanes_given_or_tuned_agree(gpu_ctx, lanes):
+    """Explicit lanes bypass the autotuner; every lane count runs the same
+    algorithm, so statuses agree and objectives within 1e-7."""
+    models = generators.batch_part1(8, count=5, m_range=(100, 500))
+    tuned = gpu_ctx.solve_batch(models, opts(1e-8))
+    fixed = gpu_ctx.solve_batch(models, opts(1e-8, lanes_per_column=lanes[0], lanes_per_row=lanes[1]))
+    for a, b in zip(tuned, fixed):
+        assert a.status == b.status == PdlpStatus.optimal
+        assert rel(a.objective, b.objective) <= 1e-7
+
+
+def test_work_queue_with_early_finishers(gpu_ctx, oracle):
+    """LPs that converge at very different iteration counts, and members
+    certified infeasible at setup, leave the work queue while the rest run on;
+    the survivors' results are those of their solo solves."""
+    bad = mcpdlp.from_triplets(1, 2, [0, 0], [0, 1], [1.0, 1.0], objective=[1.0, 1.0],
+                               var_lower=[0.0, 0.0], var_upper=[2.0, 2.0], row_lower=[5.0],
+                               row_upper=[5.0])
+    slow = generators.transport(4, 30, 40)
+    fast = synthetic("small_s7")
+    models = [fast, bad, slow, fast]
+    res = gpu_ctx.solve_batch(models, opts(1e-8))
+    assert res[1].status == PdlpStatus.infeasible_or_unbounded
+    for i in (0, 2, 3):
+        cpu = oracle.solve(models[i], options(1e-8))
+        assert res[i].status == cpu.status
+        assert rel(res[i].objective, cpu.objective) <= 1e-6
+    assert res[2].iterations > 10 * res[0].iterations
+    assert res[0].iterations == res[3].iterations and res[0].objective == res[3].objective
