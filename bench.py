@@ -286,6 +286,38 @@ def run_ncu_case(args) -> None:
     ctx.close()
 
 
+def batch_models(workload: str, world: int = 1, rank: int = 0):
+    """The batch workload's LPs of this rank (weak scaling: N ranks share a
+    batch N times the single-GPU batch, sharded by nonzeros; a rank generates
+    only the LPs of its shard)."""
+    from mcpdlp import generators
+    from mcpdlp.parallel import shard_by_nnz
+    if workload == "batch1":
+        shapes = generators.batch_part1_shapes(1, 256 * world)
+        mine = shard_by_nnz([n * k for (_, n, k) in shapes], world)[rank]
+        return (generators.batch_part1(1, 256 * world, only=mine),
+                "256 uneven LPs per GPU (m~U[100,20000], n~U[2m,4m], k~U{4..12}), batched, tolerance 1e-6")
+    mine = shard_by_nnz([1] * (512 * world), world)[rank]
+    _, models, _ = generators.batch_part2(1, 512 * world, only=mine)
+    return models, "512 node variants per GPU of one LP (m=5000, n=15000, 8 nnz/col), batched, tolerance 1e-6"
+
+
+def run_batch_ncu_case(args) -> None:
+    """A short batched solve of the batch workload (for ncu captures)."""
+    import mcpdlp
+    from mcpdlp import PdlpOptions, Precision
+    models, _ = batch_models(args.workload)
+    ctx = mcpdlp.Context(0)
+    o = PdlpOptions(max_iterations=args.ncu_iterations, profile_kernels=True,
+                    precision=Precision.fp32_refine if args.precision == "fp32_refine" else Precision.fp64)
+    o.set_tolerance(1e-6)
+    res = ctx.solve_batch(models, o)
+    print(json.dumps({"ncu_case": args.workload, "precision": args.precision,
+                      "iterations": max(r.iterations for r in res),
+                      "launches": res[0].extra["launches_by_kind"]}), flush=True)
+    ctx.close()
+
+
 def run_batch_arm(args) -> None:
     """Batched solves (one launch set for many LPs): part1 = 256 uneven LPs
     (m ~ U[100,20000], n ~ U[2m,4m], 4-12 nnz/col), part2 = 512 node variants
@@ -297,18 +329,7 @@ def run_batch_arm(args) -> None:
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     dist = init_dist(world, "nccl")
-    from mcpdlp.parallel import shard_by_nnz
-    # weak scaling: N ranks share a batch N times the single-GPU batch, sharded
-    # by nonzeros; a rank generates only the LPs of its shard
-    if args.workload == "batch1":
-        shapes = generators.batch_part1_shapes(1, 256 * world)
-        mine = shard_by_nnz([n * k for (_, n, k) in shapes], world)[rank]
-        models = generators.batch_part1(1, 256 * world, only=mine)
-        label = "256 uneven LPs per GPU (m~U[100,20000], n~U[2m,4m], k~U{4..12}), batched, tolerance 1e-6"
-    else:
-        mine = shard_by_nnz([1] * (512 * world), world)[rank]
-        _, models, _ = generators.batch_part2(1, 512 * world, only=mine)
-        label = "512 node variants per GPU of one LP (m=5000, n=15000, 8 nnz/col), batched, tolerance 1e-6"
+    models, label = batch_models(args.workload, world, rank)
     ctx = mcpdlp.Context(local)
     from mcpdlp import Precision
 
@@ -431,6 +452,15 @@ def run_engine_arm(args) -> None:
     h2d_bytes = (4 * (n + 1) + 12 * nnz + 8 * 3 * n + 8 * 2 * m)
     d2h_bytes = 8 * (n + m)
 
+    # ---- the post-solve check on the device (verify_primal, as the CLI runs it
+    # after a PDLP solve): model and candidate from host memory
+    last_e2e = e2e_res[-1]
+    t0 = time.perf_counter()
+    vrep = ctx.verify_primal(hmodel, last_e2e.primal, last_e2e.objective, TOL, TOL)
+    verify = {"s": time.perf_counter() - t0, "passed": vrep["passed"],
+              "maximum_row_violation": vrep["maximum_row_violation"],
+              "objective_difference": vrep["objective_difference"]}
+
     # ---- the mixed-precision form (FP32 iterations, FP64 checks), same LP
     from mcpdlp import Precision
     mopts = PdlpOptions(device=local, precision=Precision.fp32_refine)
@@ -501,6 +531,7 @@ def run_engine_arm(args) -> None:
         "e2e": {"value": e2e_iters / e2e_t, "unit": UNIT, "h2d_bytes_per_step": h2d_bytes,
                 "d2h_bytes_per_step": d2h_bytes, "s_per_step": e2e_t / max(1, args.steps)},
         "roofline": roofline,
+        "verify_primal_device": verify,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_reference_sample(model)
@@ -530,7 +561,10 @@ def main() -> None:
         WORKLOAD.clear()
         WORKLOAD.update(WORKLOADS[args.workload])
     if args.workload in ("batch1", "batch2"):
-        run_batch_arm(args)
+        if args.ncu_case:
+            run_batch_ncu_case(args)
+        else:
+            run_batch_arm(args)
     elif args.ncu_case:
         run_ncu_case(args)
     elif args.impl == "reference":

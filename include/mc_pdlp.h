@@ -105,12 +105,16 @@ typedef struct mc_pdlp_options {
     int32_t device;                   /* CUDA ordinal used by mc_pdlp_solve, default 0 */
     int32_t profile_kernels;          /* 1: time every kernel launch with CUDA events
                                          (no CUDA graph; slower); fills kernel_ms_by_kind */
-    int32_t refine_max_rounds;        /* FP32_REFINE: outer refinement rounds, default 12 */
-    double refine_inner_tolerance;    /* FP32_REFINE: inner relative KKT target, default 1e-4 */
+    int32_t refine_max_rounds;        /* unused (default 12): FP32_REFINE refines at every
+                                         restart, see refinement_rounds in the result */
+    double refine_inner_tolerance;    /* unused (default 1e-4), as refine_max_rounds */
     int32_t check_every_chunks;       /* host status poll interval in restart chunks, default 1 */
-    int32_t lanes_per_column;         /* A^T y kernel: 0 = chosen by mean column length,
+    int32_t lanes_per_column;         /* A^T y kernel: 0 = automatic (single LP: by mean
+                                         column length; batch: the lanes autotuner, timed on
+                                         the batch and kept per context and batch shape),
                                          -1 = one thread per column over shared-memory
-                                         tiles, 1..32 (power of two) = lanes per column */
+                                         tiles (single LP only), 1..32 (power of two) =
+                                         lanes per column */
     int32_t lanes_per_row;            /* A x kernel, same meaning per row */
     int32_t warm_start_guard;         /* 1: with a warm start, evaluate the reference's KKT score
                                          of the warm start and of the cold start (x = proj(0),
@@ -181,8 +185,9 @@ typedef struct mc_pdlp_ctx mc_pdlp_ctx;
 int mc_pdlp_abi_version(void);
 void mc_pdlp_default_options(mc_pdlp_options* options);
 
-/* sizeof of mc_lp, mc_pdlp_options, mc_pdlp_result, mc_pdlp_trace (in that
- * order) into sizes[0..count-1]; lets bindings check their struct layouts. */
+/* sizeof of mc_lp, mc_pdlp_options, mc_pdlp_result, mc_pdlp_trace,
+ * mc_verify_report (in that order) into sizes[0..count-1]; lets bindings
+ * check their struct layouts. */
 int mc_pdlp_struct_sizes(size_t* sizes, int count);
 
 /* Thread-local text of the last failure ("" if none). Returns MC_OK. */
@@ -290,6 +295,46 @@ int mc_ruiz_equilibrate(mc_pdlp_ctx* ctx, int32_t m, int32_t n, int64_t nnz,
                         double* objective, double* var_lower, double* var_upper,
                         double* row_lower, double* row_upper, int64_t max_iterations,
                         double* row_scale, double* col_scale, int64_t* iterations_executed);
+
+/*
+ * Post-solve verification of a primal candidate on the device, verify_primal
+ * at src/verify/primal_verifier.cpp:44-103 as the CLI calls it after a PDLP
+ * solve (apps/markov_cero_solve.cpp:164-168): variable bounds, row activities
+ * A x against the row bounds, and the objective recomputed and compared with
+ * the claimed one, each with an allowance abs + rel * max(1, |actual|,
+ * |expected|).  Row activities are summed in the reference's order (ascending
+ * column within each row) and, like the objective, in double-double
+ * arithmetic where the reference uses long double.  Continuous models only
+ * (mc_lp carries no integrality).
+ */
+typedef enum mc_violation_kind {
+    MC_VIOLATION_VARIABLE_LOWER = 0,
+    MC_VIOLATION_VARIABLE_UPPER = 1,
+    MC_VIOLATION_ROW_LOWER = 2,
+    MC_VIOLATION_ROW_UPPER = 3,
+    MC_VIOLATION_OBJECTIVE = 4,
+    MC_VIOLATION_KINDS = 5
+} mc_violation_kind;
+
+typedef struct mc_verify_report {
+    int32_t passed;                    /* no violation of any kind */
+    int32_t reserved0;
+    double recomputed_objective;       /* offset + sum c_j x_j (original objective) */
+    double objective_difference;       /* |recomputed - claimed| */
+    double maximum_row_violation;
+    double maximum_variable_violation;
+    int64_t violations[MC_VIOLATION_KINDS];   /* count per kind */
+    int64_t first_index[MC_VIOLATION_KINDS];  /* lowest violating index per kind, -1 if none */
+    double reserved_d[4];
+} mc_verify_report;
+
+/* primal[num_cols] in the memory the lp's `memory` field names.  Tolerances as
+ * the reference's Tolerance (finite, 0 <= value <= 1e-4, else
+ * MC_ERR_INVALID_ARGUMENT); a non-finite candidate entry or claimed objective
+ * is MC_ERR_INVALID_ARGUMENT, as the reference throws invalid_argument. */
+int mc_verify_primal(mc_pdlp_ctx* ctx, const mc_lp* lp, const double* primal, double claimed_objective,
+                     double feasibility_absolute, double feasibility_relative, double objective_absolute,
+                     double objective_relative, mc_verify_report* report);
 
 /*
  * mc_ruiz_equilibrate_noalloc: the same equilibration as mc_ruiz_equilibrate,

@@ -590,7 +590,7 @@ __global__ void __launch_bounds__(kCompactThreads) kb_compact(BatchRefs B, int* 
 // its base moves to the average and its correction data are rebuilt.
 
 template <int G>
-__global__ void __launch_bounds__(kBlock) kb_dual_mx(Iterates<float> P, MixedState M, BatchRefs B, int k) {
+__global__ void __launch_bounds__(kBlock, kMixedRowBlocks) kb_dual_mx(Iterates<float> P, MixedState M, BatchRefs B, int k) {
     const unsigned long long pol = policy_keep();
     MC_FOR_ACTIVE(B, 1, t) {
         const DevState* st = B.st + B.rows.lp[t];

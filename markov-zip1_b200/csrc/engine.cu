@@ -184,6 +184,7 @@ int pick_lanes(double mean_len) {
 #include "solve.cuh"
 #include "batch.cuh"
 #include "kernel_api.cuh"
+#include "verify.cuh"
 
 using namespace mc;
 
@@ -220,9 +221,10 @@ void mc_pdlp_default_options(mc_pdlp_options* o) {
 }
 
 int mc_pdlp_struct_sizes(size_t* sizes, int count) {
-    const size_t all[4] = {sizeof(mc_lp), sizeof(mc_pdlp_options), sizeof(mc_pdlp_result), sizeof(mc_pdlp_trace)};
+    const size_t all[5] = {sizeof(mc_lp), sizeof(mc_pdlp_options), sizeof(mc_pdlp_result), sizeof(mc_pdlp_trace),
+                           sizeof(mc_verify_report)};
     if (!sizes || count < 0) return set_error(MC_ERR_INVALID_ARGUMENT, "bad sizes buffer");
-    for (int q = 0; q < count && q < 4; ++q) sizes[q] = all[q];
+    for (int q = 0; q < count && q < 5; ++q) sizes[q] = all[q];
     return MC_OK;
 }
 

@@ -67,7 +67,7 @@ __device__ __forceinline__ void dual_update_mx(const Iterates<float>& P, const M
 }
 
 template <int G>
-__global__ void __launch_bounds__(kBlock) k_dual_mx(Iterates<float> P, MixedState M, int k) {
+__global__ void __launch_bounds__(kBlock, kMixedRowBlocks) k_dual_mx(Iterates<float> P, MixedState M, int k) {
     const DevState* st = P.st;
     if (st->done) return;
     const float sg = (float)(st->eta * st->omega);

@@ -251,6 +251,26 @@ class Context:
                                                  C.addressof(xp), C.addressof(yp), C.addressof(res)))
         return [_result_from(res[b], xs[b], ys[b]) for b in range(count)]
 
+    def verify_primal(self, model: Model, primal, claimed_objective: float,
+                      feasibility_tolerance: float = 1e-7, objective_tolerance: float = 1e-7) -> dict:
+        """verify_primal (src/verify/primal_verifier.cpp:44) on the device
+        (mc_verify_primal): absolute and relative tolerance both set to the
+        given value per kind, as the CLI does after a PDLP solve."""
+        lp = model.to_struct()
+        x = np.ascontiguousarray(primal, dtype=np.float64)
+        if x.shape != (model.num_cols,):
+            raise ValueError("candidate dimension mismatch")
+        rep = _abi.McVerifyReport()
+        _raise(self._lib.mc_verify_primal(self._h, C.addressof(lp), x.ctypes.data, float(claimed_objective),
+                                          feasibility_tolerance, feasibility_tolerance, objective_tolerance,
+                                          objective_tolerance, C.addressof(rep)))
+        return dict(passed=bool(rep.passed), recomputed_objective=rep.recomputed_objective,
+                    objective_difference=rep.objective_difference,
+                    maximum_row_violation=rep.maximum_row_violation,
+                    maximum_variable_violation=rep.maximum_variable_violation,
+                    violations={k: int(rep.violations[q]) for q, k in enumerate(_abi.VIOLATION_KINDS)},
+                    first_index={k: int(rep.first_index[q]) for q, k in enumerate(_abi.VIOLATION_KINDS)})
+
     def solve_device(self, dlp: "DeviceModel", options: Optional[PdlpOptions] = None,
                      primal_out=None, dual_out=None) -> PdlpResult:
         """solve_pdlp on a device-resident model (torch CUDA tensors); the

@@ -136,6 +136,24 @@ class McPdlpTrace(C.Structure):
     ]
 
 
+MC_VIOLATION_KINDS = 5
+VIOLATION_KINDS = ("variable_lower", "variable_upper", "row_lower", "row_upper", "objective")
+
+
+class McVerifyReport(C.Structure):
+    _fields_ = [
+        ("passed", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("recomputed_objective", C.c_double),
+        ("objective_difference", C.c_double),
+        ("maximum_row_violation", C.c_double),
+        ("maximum_variable_violation", C.c_double),
+        ("violations", C.c_int64 * MC_VIOLATION_KINDS),
+        ("first_index", C.c_int64 * MC_VIOLATION_KINDS),
+        ("reserved_d", C.c_double * 4),
+    ]
+
+
 def default_options_struct() -> McPdlpOptions:
     """Defaults of PdlpOptions (include/markov_cero/lp/first_order/pdlp.hpp:18-41)
     plus the engine extensions; identical to mc_pdlp_default_options()."""

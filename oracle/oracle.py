@@ -59,6 +59,7 @@ class CpuSolve:
     primal: np.ndarray
     dual: np.ndarray
     trace: dict | None = None
+    final_primal_weight: float = float("nan")
 
 
 def _ptr(a):
@@ -69,7 +70,7 @@ def _result(res: _abi.McPdlpResult, x, y, trace=None) -> CpuSolve:
     return CpuSolve(res.status, res.objective, res.primal_infeasibility,
                     res.dual_infeasibility, res.duality_gap, res.iterations,
                     res.message.decode(), res.total_ms, res.restarts,
-                    res.ruiz_iterations_executed, x, y, trace)
+                    res.ruiz_iterations_executed, x, y, trace, res.final_primal_weight)
 
 
 def make_trace(capacity: int):
@@ -177,6 +178,8 @@ class ReferencePdlp:
         lib.ref_mps_fetch.restype = C.c_int
         lib.ref_last_error.argtypes = [C.c_char_p, C.c_size_t]
         lib.ref_last_error.restype = C.c_int
+        lib.ref_verify_primal_report.argtypes = [_VP, _VP] + [C.c_double] * 5 + [_VP] * 4
+        lib.ref_verify_primal_report.restype = C.c_int
         lib.ref_simplex_solve.argtypes = [_VP, C.c_int64, _VP, _VP, _VP, _VP]
         lib.ref_simplex_solve.restype = C.c_int
         self.lib = lib
@@ -233,6 +236,28 @@ class ReferencePdlp:
             raise RuntimeError(f"reference simplex threw: {self._err()}")
         return dict(status=self.SIMPLEX_STATUS[st.value], objective=obj.value, primal=x,
                     iterations=it.value)
+
+    KINDS = ("variable_lower", "variable_upper", "row_lower", "row_upper", "objective")
+
+    def verify_report(self, model: Model, primal: np.ndarray, claimed: float, feasibility_tolerance: float,
+                      objective_tolerance: float) -> dict:
+        """The reference verify_primal's full report (counts and lowest index
+        per violation category), absolute = relative tolerance per kind."""
+        lp = model.to_struct()
+        x = np.ascontiguousarray(primal, dtype=np.float64)
+        counts = np.zeros(5, np.int64)
+        first = np.zeros(5, np.int64)
+        out = np.zeros(4)
+        passed = C.c_int32(0)
+        ft, ot = feasibility_tolerance, objective_tolerance
+        rc = self.lib.ref_verify_primal_report(C.addressof(lp), _ptr(x), claimed, ft, ft, ot, ot, _ptr(counts),
+                                               _ptr(first), _ptr(out), C.addressof(passed))
+        if rc != 0:
+            raise RuntimeError(f"reference verify_primal threw: {self._err()}")
+        return dict(passed=bool(passed.value), recomputed_objective=out[0], objective_difference=out[1],
+                    maximum_row_violation=out[2], maximum_variable_violation=out[3],
+                    violations={k: int(counts[q]) for q, k in enumerate(self.KINDS)},
+                    first_index={k: int(first[q]) for q, k in enumerate(self.KINDS)})
 
     def verify_primal(self, model: Model, primal: np.ndarray, claimed: float, tol: float):
         lp = model.to_struct()

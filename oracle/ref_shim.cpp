@@ -26,6 +26,7 @@
 #include <exception>
 #include <fstream>
 #include <string>
+#include <vector>
 
 namespace mdl = markov_cero::model;
 namespace fo = markov_cero::lp::first_order;
@@ -224,6 +225,42 @@ int ref_simplex_solve(const mc_lp* lp, int64_t iteration_limit, double* primal_o
             if (primal_out) std::memcpy(primal_out, x.data(), x.size() * sizeof(double));
             *objective_out = markov_cero::transform::reconstruct_objective(sparse, res.objective);
         }
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return 1;
+    }
+}
+
+// The full verify_primal report: counts and lowest index of the violations
+// per category (variable_lower, variable_upper, row_lower, row_upper,
+// objective), and recomputed objective, objective difference, maximum row and
+// variable violations in out4.
+int ref_verify_primal_report(const mc_lp* lp, const double* primal, double claimed_objective,
+                             double feas_abs, double feas_rel, double obj_abs, double obj_rel,
+                             int64_t* counts, int64_t* first, double* out4, int32_t* passed) {
+    static const char* kinds[5] = {"variable_lower", "variable_upper", "row_lower", "row_upper", "objective"};
+    try {
+        const mdl::Model model = to_model(lp);
+        markov_cero::verify::Candidate cand{
+            std::vector<double>(primal, primal + lp->num_cols), claimed_objective};
+        const markov_cero::verify::Tolerance ft{feas_abs, feas_rel}, ot{obj_abs, obj_rel};
+        const auto rep = markov_cero::verify::verify_primal(model, cand, ft, ot, 1e-6);
+        for (int k = 0; k < 5; ++k) {
+            counts[k] = 0;
+            first[k] = -1;
+        }
+        for (const auto& v : rep.violations)
+            for (int k = 0; k < 5; ++k)
+                if (v.category == kinds[k]) {
+                    counts[k] += 1;
+                    if (first[k] < 0 || (int64_t)v.index < first[k]) first[k] = (int64_t)v.index;
+                }
+        out4[0] = rep.recomputed_objective;
+        out4[1] = rep.objective_difference;
+        out4[2] = rep.maximum_row_violation;
+        out4[3] = rep.maximum_variable_violation;
+        *passed = rep.passed ? 1 : 0;
         return 0;
     } catch (const std::exception& e) {
         g_error = e.what();

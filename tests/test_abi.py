@@ -53,10 +53,11 @@ def test_library_loads_with_signatures():
 
 
 def test_struct_layouts_match():
-    sizes = (C.c_size_t * 4)()
-    assert _lib.engine().mc_pdlp_struct_sizes(sizes, 4) == 0
+    sizes = (C.c_size_t * 5)()
+    assert _lib.engine().mc_pdlp_struct_sizes(sizes, 5) == 0
     assert list(sizes) == [C.sizeof(_abi.McLp), C.sizeof(_abi.McPdlpOptions),
-                           C.sizeof(_abi.McPdlpResult), C.sizeof(_abi.McPdlpTrace)]
+                           C.sizeof(_abi.McPdlpResult), C.sizeof(_abi.McPdlpTrace),
+                           C.sizeof(_abi.McVerifyReport)]
 
 
 def test_default_options_match_reference_defaults():
