@@ -337,6 +337,26 @@ int mc_verify_primal(mc_pdlp_ctx* ctx, const mc_lp* lp, const double* primal, do
                      double objective_relative, mc_verify_report* report);
 
 /*
+ * Binary CSC model files ("MCLPCSC1": a 64-byte header, then col_start,
+ * row_index, value, objective, var_lower, var_upper, row_lower, row_upper as
+ * raw little-endian int32/double arrays; infinite bounds as IEEE infinities).
+ * They carry models past the reference MPS reader's limits
+ * (include/markov_cero/io/mps.hpp:13-20: 16 MiB, 1M rows or columns, 20M
+ * nonzeros), which the config-1 to config-3 models exceed.  No counterpart in
+ * the reference.
+ *   mc_lp_file_write: lp->memory must be MC_MEMORY_HOST.
+ *   mc_lp_file_info:  sizes from the header (the file length is checked).
+ *   mc_lp_file_read:  fills the caller's arrays, sized by lp->num_rows /
+ *     num_cols / nnz (must equal the file's), host or device per lp->memory
+ *     (device arrays on the current device: streamed through two 8 MiB pinned
+ *     buffers); sets objective_offset and objective_sense.  The arrays are
+ *     validated by the solve that uses them.
+ */
+int mc_lp_file_write(const char* path, const mc_lp* lp);
+int mc_lp_file_info(const char* path, int32_t* num_rows, int32_t* num_cols, int64_t* nnz);
+int mc_lp_file_read(const char* path, mc_lp* lp);
+
+/*
  * mc_ruiz_equilibrate_noalloc: the same equilibration as mc_ruiz_equilibrate,
  * with bit-identical results, for callers that cannot allocate device memory
  * (work inside CUDA stream capture, device memory owned by another allocator,
