@@ -312,6 +312,8 @@ int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o,
     const size_t o_off = L.add<double>(2LL * count);
     const size_t o_flags = L.add<int>(count);
     const size_t o_active = L.add<int>(2LL * kMaxTiles + 2);
+    // (x-bar, dx) pairs of the step-size iterations, in the iterate type
+    const size_t o_xdx = mixed ? L.add<float>(2LL * n) : L.add<double>(2LL * n);
     const bool tune = o->lanes_per_column == 0 || o->lanes_per_row == 0;
     size_t o_save_n[3] = {0, 0, 0}, o_save_m[2] = {0, 0};
     if (tune) {
@@ -508,6 +510,7 @@ int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o,
     P.x_bar = x_work[1];
     P.x_avg = x_work[2];
     P.dx = x_work[3];
+    P.xdx = mixed ? nullptr : static_cast<double*>(at(o_xdx));
     P.y = y_work[0];
     P.y_avg = y_work[1];
     P.ax_bar = y_work[2];
@@ -604,6 +607,7 @@ int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o,
         F.x_bar = fn[5];
         F.x_avg = fn[6];
         F.dx = fn[7];
+        F.xdx = static_cast<float*>(at(o_xdx));
         F.y = fm[1];
         F.y_avg = fm[2];
         F.ax_bar = fm[3];

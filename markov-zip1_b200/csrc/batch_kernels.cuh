@@ -91,12 +91,14 @@ __global__ void __launch_bounds__(kBlock) kb_primal(Iterates<T> P, BatchRefs B, 
                 const T tau = div_rn(step, cn);
                 const T xp = clampv(sub_rn(xo, mul_rn(tau, g)), lj, hj);
                 const T d = sub_rn(xp, xo);
+                const T xb = sub_rn(mul_rn(T(2), xp), xo);
                 if (STEP) {
-                    st_keep(P.dx + j, d, pol);
+                    st_keep2(P.xdx + 2LL * j, xb, d, pol);
                     acc += __dmul_rn(__dmul_rn((double)cn, (double)d), (double)d);
+                } else {
+                    st_keep(P.x_bar + j, xb, pol);
                 }
                 st_stream(P.x + j, xp);
-                st_keep(P.x_bar + j, sub_rn(mul_rn(T(2), xp), xo), pol);
                 st_stream(P.x_avg + j, add_rn(xa, div_rn(sub_rn(xp, xa), cnt)));
             }
         }
@@ -132,7 +134,7 @@ __global__ void __launch_bounds__(kBlock) kb_dual_probe(Iterates<T> P, BatchRefs
         double acc = 0.0;
         MC_TILE_LINES(B.rows, t, i, valid, sub) {
             T axb, adx;
-            line_dot2<G>(P.csr_start, P.csr_col, P.csr_val, P.x_bar, P.dx, i, valid, sub, axb, adx, pol);
+            line_dot2<G>(P.csr_start, P.csr_col, P.csr_val, P.xdx, i, valid, sub, axb, adx, pol);
             if (valid && sub == 0) {
                 P.ax_bar[i] = axb;
                 const double a = (double)adx;

@@ -80,6 +80,22 @@ __device__ __forceinline__ float ld_keep(const float* a, unsigned long long pol)
     asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
     return v;
 }
+// One 16-byte (8-byte for float) gather of an interleaved pair: both values
+// come from the same sector, so the pair costs one L2 request, not two.
+__device__ __forceinline__ void ld_keep2(const double* a, unsigned long long pol, double& u, double& v) {
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;"
+        : "=d"(u), "=d"(v) : "l"(a), "l"(pol));
+}
+__device__ __forceinline__ void ld_keep2(const float* a, unsigned long long pol, float& u, float& v) {
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;"
+        : "=f"(u), "=f"(v) : "l"(a), "l"(pol));
+}
+__device__ __forceinline__ void st_keep2(double* a, double u, double v, unsigned long long pol) {
+    asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(a), "d"(u), "d"(v), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void st_keep2(float* a, float u, float v, unsigned long long pol) {
+    asm volatile("st.global.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;" ::"l"(a), "f"(u), "f"(v), "l"(pol) : "memory");
+}
 __device__ __forceinline__ void st_keep(double* a, double v, unsigned long long pol) {
     asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(a), "d"(v), "l"(pol) : "memory");
 }

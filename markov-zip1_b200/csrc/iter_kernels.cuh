@@ -33,7 +33,9 @@ struct Iterates {
     T* x;                   // [n]
     T* x_bar;               // [n]
     T* x_avg;               // [n]
-    T* dx;                  // [n] step-size iterations only
+    T* dx;                  // [n] staged kernels' scratch
+    T* xdx;                 // [2n] (x-bar_j, dx_j) pairs, written on step-size iterations
+                            //      for the probe (16-byte aligned)
     T* y;                   // [m]
     T* y_avg;               // [m]
     T* ax_bar;              // [m] step-size iterations only
@@ -103,13 +105,13 @@ __device__ __forceinline__ T line_dot(const int* __restrict__ start, const int* 
     return group_sum<G>((s0 + s1) + (s2 + s3));
 }
 
-// Two dots of the same line (A x-bar and A dx on step-size iterations), two
-// entries per lane per step, both vectors gathered with the keep policy.
+// Two dots of the same line against an interleaved pair vector vw[2c] = v_c,
+// vw[2c+1] = w_c (A x-bar and A dx on step-size iterations): one gather per
+// entry brings both, two entries per lane per step.
 template <int G, class T>
 __device__ __forceinline__ void line_dot2(const int* __restrict__ start, const int* __restrict__ idx,
-                                          const T* __restrict__ val, const T* __restrict__ v,
-                                          const T* __restrict__ w, int j, bool valid, int sub,
-                                          T& out_v, T& out_w, unsigned long long pol) {
+                                          const T* __restrict__ val, const T* __restrict__ vw, int j,
+                                          bool valid, int sub, T& out_v, T& out_w, unsigned long long pol) {
     T sv0 = T(0), sw0 = T(0), sv1 = T(0), sw1 = T(0);
     if (valid) {
         const int b = __ldg(start + j), e = __ldg(start + j + 1);
@@ -117,8 +119,9 @@ __device__ __forceinline__ void line_dot2(const int* __restrict__ start, const i
         for (; p + G < e; p += 2 * G) {
             const int i0 = ld_stream(idx + p), i1 = ld_stream(idx + p + G);
             const T a0 = ld_stream(val + p), a1 = ld_stream(val + p + G);
-            const T v0 = ld_keep(v + i0, pol), v1 = ld_keep(v + i1, pol);
-            const T w0 = ld_keep(w + i0, pol), w1 = ld_keep(w + i1, pol);
+            T v0, w0, v1, w1;
+            ld_keep2(vw + 2LL * i0, pol, v0, w0);
+            ld_keep2(vw + 2LL * i1, pol, v1, w1);
             sv0 = fma(a0, v0, sv0);
             sw0 = fma(a0, w0, sw0);
             sv1 = fma(a1, v1, sv1);
@@ -127,8 +130,10 @@ __device__ __forceinline__ void line_dot2(const int* __restrict__ start, const i
         if (p < e) {
             const int i0 = ld_stream(idx + p);
             const T a0 = ld_stream(val + p);
-            sv0 = fma(a0, ld_keep(v + i0, pol), sv0);
-            sw0 = fma(a0, ld_keep(w + i0, pol), sw0);
+            T v0, w0;
+            ld_keep2(vw + 2LL * i0, pol, v0, w0);
+            sv0 = fma(a0, v0, sv0);
+            sw0 = fma(a0, w0, sw0);
         }
     }
     out_v = group_sum<G>(sv0 + sv1);
@@ -190,12 +195,14 @@ __global__ void __launch_bounds__(kBlock) k_primal(Iterates<T> P, int k) {
             const T tau = div_rn(step, cn);
             const T xp = clampv(sub_rn(xo, mul_rn(tau, g)), lj, hj);
             const T d = sub_rn(xp, xo);
-            if (STEP) {
-                st_keep(P.dx + j, d, pol);
+            const T xb = sub_rn(mul_rn(T(2), xp), xo);
+            if (STEP) {  // the probe reads x-bar and dx as pairs; x-bar alone is not read
+                st_keep2(P.xdx + 2LL * j, xb, d, pol);
                 acc += __dmul_rn(__dmul_rn((double)cn, (double)d), (double)d);
+            } else {
+                st_keep(P.x_bar + j, xb, pol);
             }
             st_stream(P.x + j, xp);
-            st_keep(P.x_bar + j, sub_rn(mul_rn(T(2), xp), xo), pol);
             st_stream(P.x_avg + j, add_rn(xa, div_rn(sub_rn(xp, xa), cnt)));
         }
     }
@@ -271,7 +278,7 @@ __global__ void __launch_bounds__(kBlock) k_dual_probe(Iterates<T> P) {
         const int i = (int)(t * LPW) + slot;
         const bool valid = i < P.m;
         T axb, adx;
-        line_dot2<G>(P.csr_start, P.csr_col, P.csr_val, P.x_bar, P.dx, i, valid, sub, axb, adx, pol);
+        line_dot2<G>(P.csr_start, P.csr_col, P.csr_val, P.xdx, i, valid, sub, axb, adx, pol);
         if (valid && sub == 0) {
             P.ax_bar[i] = axb;
             const double a = (double)adx;

@@ -597,6 +597,8 @@ int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* 
     for (auto& v : o_m) v = L.add<double>(m);
     const size_t o_partials = L.add<double>((long long)NUM_SLOTS * kMaxPartials);
     const size_t o_state = L.add<DevState>(1);
+    // (x-bar, dx) pairs of the step-size iterations, in the iterate type
+    const size_t o_xdx = mixed ? L.add<float>(2LL * n) : L.add<double>(2LL * n);
     const size_t o_tr_it = L.add<long long>(trace_cap);
     size_t o_tr[5];
     for (auto& v : o_tr) v = L.add<double>(trace_cap);
@@ -757,6 +759,7 @@ int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* 
         P.x_bar = x_bar;
         P.x_avg = x_avg;
         P.dx = dx;
+        P.xdx = static_cast<double*>(at(o_xdx));
         P.y = y;
         P.y_avg = y_avg;
         P.ax_bar = ax_bar;
@@ -824,6 +827,7 @@ int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* 
         P.x_bar = f_xb;
         P.x_avg = f_xa;
         P.dx = f_dx;
+        P.xdx = static_cast<float*>(at(o_xdx));
         P.y = f_y;
         P.y_avg = f_ya;
         P.ax_bar = f_axb;

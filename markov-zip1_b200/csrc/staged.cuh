@@ -96,24 +96,26 @@ __device__ __forceinline__ T seq_dot(const int* idx, const T* val, int b, int e,
 
 // Same, two vectors at once (A x-bar and A dx).
 template <class T>
-__device__ __forceinline__ void seq_dot2(const int* idx, const T* val, int b, int e, const T* __restrict__ v,
-                                         const T* __restrict__ w, unsigned long long pol, T& sv, T& sw) {
+__device__ __forceinline__ void seq_dot2(const int* idx, const T* val, int b, int e, const T* __restrict__ vw,
+                                         unsigned long long pol, T& sv, T& sw) {
     sv = T(0);
     sw = T(0);
     int p = b;
     for (; p + 2 <= e; p += 2) {
         const int i0 = idx[p], i1 = idx[p + 1];
-        const T v0 = ld_keep(v + i0, pol), v1 = ld_keep(v + i1, pol);
-        const T w0 = ld_keep(w + i0, pol), w1 = ld_keep(w + i1, pol);
+        T v0, w0, v1, w1;
+        ld_keep2(vw + 2LL * i0, pol, v0, w0);
+        ld_keep2(vw + 2LL * i1, pol, v1, w1);
         sv = add_rn(sv, mul_rn(val[p], v0));
         sw = add_rn(sw, mul_rn(val[p], w0));
         sv = add_rn(sv, mul_rn(val[p + 1], v1));
         sw = add_rn(sw, mul_rn(val[p + 1], w1));
     }
     if (p < e) {
-        const int i0 = idx[p];
-        sv = add_rn(sv, mul_rn(val[p], ld_keep(v + i0, pol)));
-        sw = add_rn(sw, mul_rn(val[p], ld_keep(w + i0, pol)));
+        T v0, w0;
+        ld_keep2(vw + 2LL * idx[p], pol, v0, w0);
+        sv = add_rn(sv, mul_rn(val[p], v0));
+        sw = add_rn(sw, mul_rn(val[p], w0));
     }
 }
 
@@ -195,12 +197,14 @@ __global__ void __launch_bounds__(kBlock) k_primal_staged(Iterates<T> P, Tiles T
                         const T xo = ld_stream(P.x + j);
                         const T xp = clampv(sub_rn(xo, mul_rn(tau, g)), ld_stream(P.lo + j), ld_stream(P.hi + j));
                         const T d = sub_rn(xp, xo);
+                        const T xb = sub_rn(mul_rn(T(2), xp), xo);
                         if (STEP) {
-                            st_keep(P.dx + j, d, keep);
+                            st_keep2(P.xdx + 2LL * j, xb, d, keep);
                             acc += __dmul_rn(__dmul_rn((double)cn, (double)d), (double)d);
+                        } else {
+                            st_keep(P.x_bar + j, xb, keep);
                         }
                         st_stream(P.x + j, xp);
-                        st_keep(P.x_bar + j, sub_rn(mul_rn(T(2), xp), xo), keep);
                         const T xa = ld_stream(P.x_avg + j);
                         st_stream(P.x_avg + j, add_rn(xa, div_rn(sub_rn(xp, xa), cnt)));
                     });
@@ -236,7 +240,7 @@ __global__ void __launch_bounds__(kBlock) k_dual_probe_staged(Iterates<T> P, Til
     stream_lines<T>(Tl.row_bounds, Tl.nrow_tiles, P.csr_start, P.csr_col, P.csr_val,
                     [&](int i, const int* idx, const T* val, int b, int e) {
                         T axb, adx;
-                        seq_dot2(idx, val, b, e, P.x_bar, P.dx, keep, axb, adx);
+                        seq_dot2(idx, val, b, e, P.xdx, keep, axb, adx);
                         P.ax_bar[i] = axb;
                         const double a = (double)adx;
                         acc += __ddiv_rn(__dmul_rn(a, a), (double)P.row_norm[i]);
