@@ -296,6 +296,23 @@ int mc_ruiz_equilibrate(mc_pdlp_ctx* ctx, int32_t m, int32_t n, int64_t nnz,
                         double* row_lower, double* row_upper, int64_t max_iterations,
                         double* row_scale, double* col_scale, int64_t* iterations_executed);
 
+/* The simplex path's equilibration of a canonical model (SparseCanonicalModel
+ * CSC, rhs, objective) on the device: equilibrate at
+ * src/scale/ruiz_scaling.cpp:20-125.  The same Ruiz loop as above with the
+ * given tolerance, then the scales clamped to [min_scale, max_scale] (values
+ * keep the unclamped scaling, as in the reference), their inverses, rhs[m]
+ * scaled by the row scales and objective[n] by the column scales.  An empty
+ * model (m, n or nnz 0) gets unit scales and untouched rhs/objective.  A
+ * non-finite scaled rhs/objective is MC_ERR_INVALID_ARGUMENT (the reference
+ * throws overflow_error).  Device arrays; reference defaults: 10 passes,
+ * tolerance 1e-3, scales in [1e-4, 1e4]. */
+int mc_ruiz_equilibrate_canonical(mc_pdlp_ctx* ctx, int32_t m, int32_t n, int64_t nnz,
+                                  const int32_t* col_start, const int32_t* row_index, double* value,
+                                  double* rhs, double* objective, int64_t max_iterations, double tolerance,
+                                  double min_scale, double max_scale, double* row_scale, double* col_scale,
+                                  double* inv_row_scale, double* inv_col_scale, int64_t* iterations_executed,
+                                  int32_t* converged);
+
 /*
  * Post-solve verification of a primal candidate on the device, verify_primal
  * at src/verify/primal_verifier.cpp:44-103 as the CLI calls it after a PDLP

@@ -179,7 +179,8 @@ int build_csr(Ctx& ctx, int m, int n, long long nnz, const int* csc_start, const
 // ------------------------------------------------------------------ Ruiz
 int ruiz(Ctx& ctx, int m, int n, long long nnz, const int* csc_start, const int* csc_row, double* csc_val,
          const int* csr_start, const int* csr_col, double* csr_val, double* row_scale, double* col_scale,
-         double* r_tmp, double* c_tmp, double* partials, DevState* st, long long passes) {
+         double* r_tmp, double* c_tmp, double* partials, DevState* st, long long passes,
+         double tolerance = 1e-3) {
     cudaStream_t s = ctx.stream;
     ctx.begin_launch(MC_KERNEL_SETUP);
     k_fill<double><<<blocks_for(ctx, m, kBlock), kBlock, 0, s>>>(row_scale, m, 1.0);
@@ -198,7 +199,7 @@ int ruiz(Ctx& ctx, int m, int n, long long nnz, const int* csc_start, const int*
         ctx.end_launch();
         ctx.begin_launch(MC_KERNEL_SETUP);
         k_ruiz_check<<<1, 1024, 0, s>>>(partials + SLOT_B * kMaxPartials, nbr, partials + SLOT_A * kMaxPartials,
-                                        nbc, 1e-3, st);
+                                        nbc, tolerance, st);
         ctx.end_launch();
         ctx.begin_launch(MC_KERNEL_SETUP);
         k_ruiz_deltas<<<nbr, kBlock, 0, s>>>(m, r_tmp, row_scale, st);

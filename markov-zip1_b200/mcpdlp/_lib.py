@@ -68,6 +68,8 @@ ENGINE_SIGNATURES = {
     "mc_lp_file_write": ([C.c_char_p, _VP], C.c_int),
     "mc_lp_file_info": ([C.c_char_p, _VP, _VP, _VP], C.c_int),
     "mc_lp_file_read": ([C.c_char_p, _VP], C.c_int),
+    "mc_ruiz_equilibrate_canonical": ([_VP, _I32, _I32, _I64, _VP, _VP, _VP, _VP, _VP, _I64, C.c_double,
+                                       C.c_double, C.c_double, _VP, _VP, _VP, _VP, _VP, _VP], C.c_int),
     "mc_verify_primal": ([_VP, _VP, _VP, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, _VP],
                          C.c_int),
     "mc_ruiz_equilibrate_noalloc": ([_I32, _I32, _I64, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP,

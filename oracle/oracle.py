@@ -180,6 +180,10 @@ class ReferencePdlp:
         lib.ref_last_error.restype = C.c_int
         lib.ref_verify_primal_report.argtypes = [_VP, _VP] + [C.c_double] * 5 + [_VP] * 4
         lib.ref_verify_primal_report.restype = C.c_int
+        lib.ref_canonical_sizes.argtypes = [_VP, _VP, _VP, _VP]
+        lib.ref_canonical_sizes.restype = C.c_int
+        lib.ref_canonical_equilibrate.argtypes = [C.c_int64] + [C.c_double] * 3 + [_VP] * 14
+        lib.ref_canonical_equilibrate.restype = C.c_int
         lib.ref_simplex_solve.argtypes = [_VP, C.c_int64, _VP, _VP, _VP, _VP]
         lib.ref_simplex_solve.restype = C.c_int
         self.lib = lib
@@ -258,6 +262,31 @@ class ReferencePdlp:
                     maximum_row_violation=out[2], maximum_variable_violation=out[3],
                     violations={k: int(counts[q]) for q, k in enumerate(self.KINDS)},
                     first_index={k: int(first[q]) for q, k in enumerate(self.KINDS)})
+
+    def canonical_equilibrate(self, model: Model, max_iterations: int = 10, tolerance: float = 1e-3,
+                              min_scale: float = 1e-4, max_scale: float = 1e4) -> dict:
+        """The CLI's canonical model of `model` (sparse_canonicalize) before and
+        after the reference's equilibrate (src/scale/ruiz_scaling.cpp:20-125)."""
+        lp = model.to_struct()
+        m, n, z = C.c_int64(), C.c_int64(), C.c_int64()
+        if self.lib.ref_canonical_sizes(C.addressof(lp), C.addressof(m), C.addressof(n), C.addressof(z)) != 0:
+            raise RuntimeError(f"reference sparse_canonicalize threw: {self._err()}")
+        m, n, z = m.value, n.value, z.value
+        out = dict(m=m, n=n, nnz=z, col_start=np.zeros(n + 1, np.int32), row_index=np.zeros(z, np.int32))
+        for k, size in (("value_in", z), ("rhs_in", m), ("objective_in", n), ("value", z), ("rhs", m),
+                        ("objective", n), ("row_scale", m), ("col_scale", n), ("inv_row_scale", m),
+                        ("inv_col_scale", n)):
+            out[k] = np.zeros(size)
+        it, conv = C.c_int64(), C.c_int32()
+        rc = self.lib.ref_canonical_equilibrate(
+            max_iterations, tolerance, min_scale, max_scale, _ptr(out["col_start"]), _ptr(out["row_index"]),
+            _ptr(out["value_in"]), _ptr(out["rhs_in"]), _ptr(out["objective_in"]), _ptr(out["value"]),
+            _ptr(out["rhs"]), _ptr(out["objective"]), _ptr(out["row_scale"]), _ptr(out["col_scale"]),
+            _ptr(out["inv_row_scale"]), _ptr(out["inv_col_scale"]), C.addressof(it), C.addressof(conv))
+        if rc != 0:
+            raise RuntimeError(f"reference equilibrate threw: {self._err()}")
+        out["iterations"], out["converged"] = it.value, bool(conv.value)
+        return out
 
     def verify_primal(self, model: Model, primal: np.ndarray, claimed: float, tol: float):
         lp = model.to_struct()

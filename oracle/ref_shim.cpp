@@ -268,6 +268,63 @@ int ref_verify_primal_report(const mc_lp* lp, const double* primal, double claim
     }
 }
 
+// The canonical model of an LP (sparse_canonicalize, as the CLI's simplex
+// path builds it) and the reference's equilibrate on it
+// (src/scale/ruiz_scaling.cpp:20-125).  ref_canonical_sizes gives m, n, nnz;
+// ref_canonical_equilibrate writes the canonical CSC and rhs/objective before
+// scaling (col_start, row_index, value_in, rhs_in, obj_in) and the results.
+thread_local markov_cero::transform::SparseCanonicalModel g_canonical;
+
+int ref_canonical_sizes(const mc_lp* lp, int64_t* m, int64_t* n, int64_t* nnz) {
+    try {
+        g_canonical = markov_cero::transform::sparse_canonicalize(to_model(lp), /*relax_integrality=*/true);
+        *m = (int64_t)g_canonical.matrix.rows;
+        *n = (int64_t)g_canonical.matrix.columns;
+        *nnz = (int64_t)g_canonical.matrix.values.size();
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return 1;
+    }
+}
+
+int ref_canonical_equilibrate(int64_t max_iterations, double tolerance, double min_scale, double max_scale,
+                              int32_t* col_start, int32_t* row_index, double* value_in, double* rhs_in,
+                              double* obj_in, double* value_out, double* rhs_out, double* obj_out,
+                              double* row_scale, double* col_scale, double* inv_row, double* inv_col,
+                              int64_t* iterations, int32_t* converged) {
+    try {
+        auto& c = g_canonical;
+        const std::size_t m = c.matrix.rows, n = c.matrix.columns, z = c.matrix.values.size();
+        for (std::size_t j = 0; j <= n; ++j) col_start[j] = (int32_t)c.matrix.column_offsets[j];
+        for (std::size_t p = 0; p < z; ++p) {
+            row_index[p] = (int32_t)c.matrix.row_indices[p];
+            value_in[p] = c.matrix.values[p];
+        }
+        std::memcpy(rhs_in, c.rhs.data(), m * sizeof(double));
+        std::memcpy(obj_in, c.objective.data(), n * sizeof(double));
+        markov_cero::scale::RuizOptions ro;
+        ro.max_iterations = (std::size_t)max_iterations;
+        ro.tolerance = tolerance;
+        ro.min_scale = min_scale;
+        ro.max_scale = max_scale;
+        const auto sc = markov_cero::scale::equilibrate(c, ro);
+        std::memcpy(value_out, c.matrix.values.data(), z * sizeof(double));
+        std::memcpy(rhs_out, c.rhs.data(), m * sizeof(double));
+        std::memcpy(obj_out, c.objective.data(), n * sizeof(double));
+        std::memcpy(row_scale, sc.row_scale.data(), m * sizeof(double));
+        std::memcpy(col_scale, sc.col_scale.data(), n * sizeof(double));
+        std::memcpy(inv_row, sc.inv_row_scale.data(), m * sizeof(double));
+        std::memcpy(inv_col, sc.inv_col_scale.data(), n * sizeof(double));
+        *iterations = (int64_t)sc.iterations_executed;
+        *converged = sc.converged ? 1 : 0;
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return 1;
+    }
+}
+
 // Parse an MPS file with the reference parser; sizes first, arrays by fetch.
 int ref_mps_load(const char* path, int32_t* m, int32_t* n, int64_t* nnz, int32_t* sense,
                  double* offset) {

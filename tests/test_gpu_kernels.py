@@ -135,3 +135,36 @@ def test_spmv_matches_oracle(gpu_ctx, oracle, name):
         for p in range(m.col_start[j], m.col_start[j + 1]):
             absum[m.row_index[p]] += abs(m.value[p] * x[j])
     assert np.all(np.abs(got - expect) <= 1e-13 * np.maximum(absum, 1e-300))
+
+
+CANONICAL_OPTIONS = [dict(), dict(min_scale=0.5, max_scale=2.0), dict(tolerance=0.5), dict(max_iterations=3)]
+
+
+@pytest.mark.parametrize("name", ["netlib_afiro", "small_s7", "precision_s1", "transport"])
+@pytest.mark.parametrize("opt", range(len(CANONICAL_OPTIONS)))
+def test_canonical_ruiz_bit_exact(gpu_ctx, reference, name, opt):
+    """mc_ruiz_equilibrate_canonical against the reference's equilibrate
+    (src/scale/ruiz_scaling.cpp:20-125) on the CLI's canonical model of the LP:
+    values, rhs, objective, clamped scales, inverses, pass count, converged.
+    (The reference's sparse canonical form caps the model size, so the LPs are
+    the small golden ones.)"""
+    import torch
+    from test_oracle import load_model
+    m = (generators.transport(2, 20, 30) if name == "transport" else
+         load_model(name) if name.startswith("netlib") else synthetic(name))
+    kw = dict(max_iterations=10, tolerance=1e-3, min_scale=1e-4, max_scale=1e4)
+    kw.update(CANONICAL_OPTIONS[opt])
+    ref = reference.canonical_equilibrate(m, **kw)
+    cm, cn, nnz = ref["m"], ref["n"], ref["nnz"]
+    cs, ri, v = dev(ref["col_start"]), dev(ref["row_index"]), dev(ref["value_in"])
+    rhs, obj = dev(ref["rhs_in"]), dev(ref["objective_in"])
+    scales = [torch.zeros(k, dtype=torch.float64, device="cuda") for k in (cm, cn, cm, cn)]
+    it, conv = C.c_int64(-1), C.c_int32(-1)
+    _lib.check(_lib.engine().mc_ruiz_equilibrate_canonical(
+        gpu_ctx.handle, cm, cn, nnz, cs.data_ptr(), ri.data_ptr(), v.data_ptr(), rhs.data_ptr(), obj.data_ptr(),
+        kw["max_iterations"], kw["tolerance"], kw["min_scale"], kw["max_scale"], *[t.data_ptr() for t in scales],
+        C.addressof(it), C.addressof(conv)))
+    assert it.value == ref["iterations"] and bool(conv.value) == ref["converged"]
+    for t, k in ((v, "value"), (rhs, "rhs"), (obj, "objective"), (scales[0], "row_scale"),
+                 (scales[1], "col_scale"), (scales[2], "inv_row_scale"), (scales[3], "inv_col_scale")):
+        assert np.array_equal(t.cpu().numpy(), ref[k]), k
