@@ -37,7 +37,7 @@ struct TileTable {
     int ntiles;
 };
 
-constexpr int kMaxTiles = 1 << 17;  // per-slot capacity of the batch partials buffer
+constexpr int kMaxTiles = 1 << 18;  // per-slot capacity of the batch partials buffer
 
 struct BatchRefs {
     DevState* st;              // [nlp]
@@ -533,13 +533,17 @@ __global__ void kb_shift_indices(int* __restrict__ col_start, int* __restrict__ 
     }
 }
 
-// The work queue (one block of kCompactThreads): the running column and row
-// tiles in table order, and the packed loop's poll flag (done once every LP is
-// done).  An ordered compaction: ballots give each warp's survivors, a scan
-// of the warp totals their offsets.
+// The work queue, rebuilt after every check in two launches.  An LP's tiles
+// are contiguous and an LP is either running or done, so the running tiles
+// are the tile ranges of the running LPs, in LP order:
+//   kb_compact (one block): offsets of each LP's range in the two lists (an
+//     exclusive scan over the LPs), the list lengths, and the packed loop's
+//     poll flag (done once every LP is done);
+//   kb_fill_active (one thread per tile): a running LP's tile t goes to
+//     position offset(LP) + (t - first tile of the LP).
 constexpr int kCompactThreads = 1024;
 
-__global__ void __launch_bounds__(kCompactThreads) kb_compact(BatchRefs B, int* __restrict__ active,
+__global__ void __launch_bounds__(kCompactThreads) kb_compact(BatchRefs B, int* __restrict__ lp_offset,
                                                               int* __restrict__ active_count,
                                                               DevState* __restrict__ global) {
     __shared__ int warp_total[32];
@@ -547,42 +551,61 @@ __global__ void __launch_bounds__(kCompactThreads) kb_compact(BatchRefs B, int* 
     __shared__ int running;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int kWarps = kCompactThreads / 32;
+    if (threadIdx.x == 0) running = 0;
     for (int which = 0; which < 2; ++which) {
         const TileTable& T = which ? B.rows : B.cols;
-        int* out = active + which * kMaxTiles;
+        int* off = lp_offset + which * (B.nlp + 1);
         if (threadIdx.x == 0) base = 0;
         __syncthreads();
-        for (int t0 = 0; t0 < T.ntiles; t0 += kCompactThreads) {
-            const int t = t0 + threadIdx.x;
-            const bool keep = t < T.ntiles && !B.st[T.lp[t]].done;
-            const unsigned ballot = __ballot_sync(0xffffffffu, keep);
-            if (lane == 0) warp_total[warp] = __popc(ballot);
+        for (int b0 = 0; b0 < B.nlp; b0 += kCompactThreads) {
+            const int b = b0 + threadIdx.x;
+            const bool run = b < B.nlp && !B.st[b].done;
+            const int cnt = run ? T.first[b + 1] - T.first[b] : 0;
+            if (which == 0 && run) atomicAdd(&running, 1);
+            int v = cnt;  // inclusive scan within the warp
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int u = __shfl_up_sync(0xffffffffu, v, d);
+                if (lane >= d) v += u;
+            }
+            if (lane == 31) warp_total[warp] = v;
             __syncthreads();
             if (warp == 0) {
-                int v = warp_total[lane];
+                int w = warp_total[lane];
 #pragma unroll
-                for (int off = 1; off < 32; off <<= 1) {
-                    const int u = __shfl_up_sync(0xffffffffu, v, off);
-                    if (lane >= off) v += u;
+                for (int d = 1; d < 32; d <<= 1) {
+                    const int u = __shfl_up_sync(0xffffffffu, w, d);
+                    if (lane >= d) w += u;
                 }
-                warp_total[lane] = v;  // inclusive prefix over warps
+                warp_total[lane] = w;  // inclusive prefix over warps
             }
             __syncthreads();
-            if (keep) out[base + (warp ? warp_total[warp - 1] : 0) + __popc(ballot & ((1u << lane) - 1u))] = t;
+            const int excl = base + (warp ? warp_total[warp - 1] : 0) + v - cnt;
+            if (b < B.nlp) off[b] = excl;
             __syncthreads();
             if (threadIdx.x == 0) base += warp_total[kWarps - 1];
             __syncthreads();
         }
-        if (threadIdx.x == 0) active_count[which] = base;
+        if (threadIdx.x == 0) {
+            off[B.nlp] = base;
+            active_count[which] = base;
+            global->active_tiles[which] = base;  // read by the host's poll
+        }
         __syncthreads();
     }
-    if (threadIdx.x == 0) running = 0;
-    __syncthreads();
-    int c = 0;
-    for (int b = threadIdx.x; b < B.nlp; b += blockDim.x) c += B.st[b].done ? 0 : 1;
-    if (c) atomicAdd(&running, c);
-    __syncthreads();
     if (threadIdx.x == 0) global->done = running == 0 ? 1 : 0;
+}
+
+__global__ void __launch_bounds__(kBlock) kb_fill_active(BatchRefs B, const int* __restrict__ lp_offset,
+                                                         int* __restrict__ active) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= B.cols.ntiles + B.rows.ntiles) return;
+    const int which = q < B.cols.ntiles ? 0 : 1;
+    const int t = which ? q - B.cols.ntiles : q;
+    const TileTable& T = which ? B.rows : B.cols;
+    const int lp = T.lp[t];
+    if (B.st[lp].done) return;
+    active[which * kMaxTiles + lp_offset[which * (B.nlp + 1) + lp] + (t - T.first[lp])] = t;
 }
 
 // ------------------------------------------------- mixed precision, batched

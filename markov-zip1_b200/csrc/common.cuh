@@ -53,7 +53,8 @@ struct DevState {
     int restart_pending;            // finalize -> restart copy
     int ruiz_done;                  // Ruiz converged: later passes are no-ops
     int nonfinite;                  // a residual pass saw NaN/Inf
-    int pad[3];
+    int active_tiles[2];            // batch poll state: running column / row tiles
+    int pad;
 };
 
 // ---- cache policy helpers -------------------------------------------------

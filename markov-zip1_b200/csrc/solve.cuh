@@ -222,6 +222,10 @@ int ruiz(Ctx& ctx, int m, int n, long long nnz, const int* csc_start, const int*
 // the fused kernels on the iterate itself; the mixed form runs the FP32
 // kernels on the correction and checks in FP64 (mixed.cuh).
 struct Engine64 {
+    // one launch shape per solve (the batch engines vary theirs)
+    int shape_class(const DevState&) const { return 0; }
+    void use_class(int) const {}
+
     Iterates<double> P;
     Original O;
     Plan pl;
@@ -287,6 +291,10 @@ struct Engine64 {
 };
 
 struct EngineMixed {
+    // one launch shape per solve (the batch engines vary theirs)
+    int shape_class(const DevState&) const { return 0; }
+    void use_class(int) const {}
+
     Iterates<float> P;
     MixedState M;
     Original O;
@@ -363,8 +371,7 @@ int enqueue_span(Ctx& ctx, const E& eng, long long base, int k0, int k1, const C
 // schedule of step-size iterations depends only on base % 10.
 template <class E>
 int chunk_graph(Ctx& ctx, const E& eng, long long base, long long R, const Controls& ctl, const TraceBuf& tr,
-                cudaGraphExec_t* out, long long recipe[MC_KERNEL_KINDS]) {
-    const int key = (int)(base % 10);
+                int key, cudaGraphExec_t* out, long long recipe[MC_KERNEL_KINDS]) {
     long long before[MC_KERNEL_KINDS];
     std::memcpy(before, ctx.launches, sizeof before);
     CU(cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeThreadLocal));
@@ -403,21 +410,24 @@ int run_chunks(Ctx& ctx, const E& eng, DevState* st, long long maxit, long long 
     const long long full_chunks = maxit / R;
     long long base = 0;
     bool done = false;
-    long long recipe[10][MC_KERNEL_KINDS] = {};
+    long long recipe[40][MC_KERNEL_KINDS] = {};
     int inflight = 0;
     int ev_idx = 0;
     bool have_prev = false;
+    int cls = 0;  // the engine's launch-shape class, from the last poll
     for (long long chunk = 0; chunk < full_chunks && !done; ++chunk) {
+        eng.use_class(cls);
         if (ctx.profiling) {
             TRY(enqueue_span(ctx, eng, base, 0, (int)R, ctl));
             TRY(eng.check(ctx, R, 0, ctl, tr));
             TRY(ctx.drain_profile());
         } else {
-            const int key = (int)(base % 10);
+            // graphs keyed by the step-size phase (base % 10) and the class
+            const int key = (int)(base % 10) + 10 * cls;
             auto it = ctx.graphs.find(key);
             cudaGraphExec_t exec = nullptr;
             if (it == ctx.graphs.end()) {
-                TRY(chunk_graph(ctx, eng, base, R, ctl, tr, &exec, recipe[key]));
+                TRY(chunk_graph(ctx, eng, base, R, ctl, tr, key, &exec, recipe[key]));
             } else {
                 exec = it->second;
             }
@@ -430,6 +440,7 @@ int run_chunks(Ctx& ctx, const E& eng, DevState* st, long long maxit, long long 
             if (have_prev) {
                 CU(cudaEventSynchronize(ctx.ev_poll[ev_idx ^ 1]));
                 if (ctx.h_state[ev_idx ^ 1].done) done = true;
+                cls = eng.shape_class(ctx.h_state[ev_idx ^ 1]);
             }
             CU(cudaMemcpyAsync(&ctx.h_state[ev_idx], st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
             CU(cudaEventRecord(ctx.ev_poll[ev_idx], s));
