@@ -18,9 +18,11 @@ Writes, next to this script:
                    generated arrays), equilibrate_model digests, and the
                    reference primal simplex's optimum of small seeded
                    transportation LPs (the FP64 optimum of that family, which
-                   has no analytic one).
+                   has no analytic one), and the published optimal objectives of
+                   the Netlib fixtures (the reference's scripts/run_netlib.py).
 
     python tests/golden/make_golden.py --only simplex   # refresh that section
+    python tests/golden/make_golden.py --only netlib    # the published Netlib optima
 """
 from __future__ import annotations
 
@@ -109,6 +111,17 @@ def record(ref, m: Model) -> dict:
     return out
 
 
+def netlib_optima() -> dict:
+    """The published Netlib optimal objectives the reference's benchmark
+    script carries (scripts/run_netlib.py:19-93), for the fixtures here."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("run_netlib", REF / "scripts" / "run_netlib.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return {f"netlib_{k}": float(v["optimal"]) for k, v in mod.NETLIB_BENCHMARKS.items()
+            if k in NETLIB and "optimal" in v}
+
+
 def simplex_section(ref) -> dict:
     out = {}
     for seed, S, D in TRANSPORT:
@@ -128,9 +141,13 @@ def simplex_section(ref) -> dict:
 def main() -> None:
     orc.build(reference=True)
     ref = orc.ReferencePdlp()
-    if "--only" in sys.argv and sys.argv[sys.argv.index("--only") + 1] == "simplex":
+    if "--only" in sys.argv:
         golden = json.loads((HERE / "golden.json").read_text())
-        golden["simplex"] = simplex_section(ref)
+        what = sys.argv[sys.argv.index("--only") + 1]
+        if what == "simplex":
+            golden["simplex"] = simplex_section(ref)
+        elif what == "netlib":
+            golden["netlib_optimal"] = netlib_optima()
         (HERE / "golden.json").write_text(json.dumps(golden, indent=1, sort_keys=True))
         return
     golden = {"models": {}, "synthetic": {}, "ruiz": {}}
@@ -160,6 +177,7 @@ def main() -> None:
                                     bounds_sha256=sha(e["objective"], e["var_lower"], e["var_upper"],
                                                       e["row_lower"], e["row_upper"]))
     golden["simplex"] = simplex_section(ref)
+    golden["netlib_optimal"] = netlib_optima()
     (HERE / "golden.json").write_text(json.dumps(golden, indent=1, sort_keys=True))
 
 

@@ -249,3 +249,19 @@ def test_transport_against_simplex_optimum(gpu_ctx, name):
         assert rel(res.objective, g["objective"]) <= 1e-4
         if res.status == PdlpStatus.optimal:
             assert rel(res.objective, g["objective"]) <= 1e-6
+
+
+NETLIB_CASES = [(n, "fp64") for n in sorted(GOLDEN["netlib_optimal"])] + [
+    (n, "fp32_refine") for n in ("netlib_afiro", "netlib_sc50a", "netlib_sc50b")]
+
+
+@pytest.mark.parametrize("name,precision", NETLIB_CASES)
+def test_netlib_published_optima(gpu_ctx, name, precision):
+    """Known answers: the published Netlib optima (the reference's
+    scripts/run_netlib.py:19-93) at 1e-8 relative KKT (the mixed form on the
+    models its own tests cover)."""
+    from mcpdlp import Precision
+    res = gpu_ctx.solve(load_model(name), gpu_opts(1e-8, precision=Precision[precision]))
+    best = GOLDEN["netlib_optimal"][name]
+    assert res.status == PdlpStatus.optimal
+    assert abs(res.objective - best) <= 1e-6 * max(1.0, abs(best)), (res.objective, best)

@@ -221,3 +221,13 @@ def test_oracle_pdlp_against_simplex_optimum(oracle, name):
                                                      g["pdlp_1e8"]["objective"])
     if r.status == 0:
         assert abs(r.objective - g["objective"]) <= 1e-6 * abs(g["objective"])
+
+
+@pytest.mark.parametrize("name", ["netlib_afiro", "netlib_sc50a", "netlib_sc50b"])
+def test_oracle_reaches_published_netlib_optima(oracle, name):
+    """Known answers: the published Netlib optima (the reference's
+    scripts/run_netlib.py:19-93), reached by the PDLP at 1e-8 within 1e-6."""
+    r = oracle.solve(load_model(name), options(1e-8))
+    best = GOLDEN["netlib_optimal"][name]
+    assert r.status == 0
+    assert abs(r.objective - best) <= 1e-6 * max(1.0, abs(best))
