@@ -241,6 +241,19 @@ int mc_pdlp_ctx_solve_batch(mc_pdlp_ctx* ctx, const mc_lp* lps, int32_t count,
                             const mc_pdlp_options* options, double* const* primal_out,
                             double* const* dual_out, mc_pdlp_result* results);
 
+/* The batched solve with a starting point per LP, as initial_primal /
+ * initial_dual of mc_pdlp_ctx_solve (original space; projected onto the
+ * bounds): initial_primal[b] (num_cols of LP b) and initial_dual[b] (num_rows),
+ * either array or any entry NULL for a cold start of that part.  Branch and
+ * bound passes each node the parent's solution.  No guard: the start is used
+ * as given (warm_start_guard is ignored).  No counterpart in the reference,
+ * whose node LPs warm-start the dual simplex from the parent's basis
+ * (src/milp/node_lp.cpp:44-60). */
+int mc_pdlp_ctx_solve_batch_warm(mc_pdlp_ctx* ctx, const mc_lp* lps, int32_t count,
+                                 const mc_pdlp_options* options, const double* const* initial_primal,
+                                 const double* const* initial_dual, double* const* primal_out,
+                                 double* const* dual_out, mc_pdlp_result* results);
+
 /*
  * Learned warm start (no counterpart in the reference): a bipartite
  * message-passing network over an LP's constraint/variable graph (hidden 64,

@@ -280,8 +280,8 @@ static void make_tiles(const std::vector<long long>& off, int per_tile, std::vec
     first[nlp] = (int)lp.size();
 }
 
-int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o, double* const* x_out,
-                double* const* y_out, mc_pdlp_result* results) {
+int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o, const double* const* x0,
+                const double* const* y0, double* const* x_out, double* const* y_out, mc_pdlp_result* results) {
     const double t_begin = now_ms();
     if (!lps || count <= 0 || !results) return set_error(MC_ERR_INVALID_ARGUMENT, "empty batch");
     TRY(validate_options(o));
@@ -336,6 +336,12 @@ int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o,
     const size_t o_st = L.add<DevState>(count + 1);
     const size_t o_off = L.add<double>(2LL * count);
     const size_t o_flags = L.add<int>(count);
+    bool any_warm = false;
+    for (int b = 0; b < count; ++b)
+        any_warm = any_warm || (x0 && x0[b] && lps[b].num_cols > 0) || (y0 && y0[b] && lps[b].num_rows > 0);
+    const size_t o_warm = any_warm ? L.add<int>(count) : 0;
+    const size_t o_warm_x = any_warm ? L.add<double>(n) : 0;
+    const size_t o_warm_y = any_warm ? L.add<double>(m) : 0;
     const size_t o_active = L.add<int>(2LL * kMaxTiles + 2);
     const size_t o_lp_offset = L.add<int>(2LL * (count + 1));
     // (x-bar, dx) pairs of the step-size iterations, in the iterate type
@@ -436,6 +442,22 @@ int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o,
         const int total = (int)nnz;
         CU(cudaMemcpyAsync(cs + n, &total, sizeof(int), cudaMemcpyHostToDevice, s));
     }
+    // starting points: packed like the model, a flag per LP says which parts exist
+    int* warm = any_warm ? static_cast<int*>(at(o_warm)) : nullptr;
+    double* warm_x = any_warm ? static_cast<double*>(at(o_warm_x)) : nullptr;
+    double* warm_y = any_warm ? static_cast<double*>(at(o_warm_y)) : nullptr;
+    std::vector<int> warm_host(any_warm ? count : 0, 0);
+    for (int b = 0; b < count && any_warm; ++b) {
+        if (x0 && x0[b] && lps[b].num_cols > 0) {
+            warm_host[b] |= 1;
+            CU(cudaMemcpyAsync(warm_x + col_off[b], x0[b], sizeof(double) * lps[b].num_cols, cudaMemcpyDefault, s));
+        }
+        if (y0 && y0[b] && lps[b].num_rows > 0) {
+            warm_host[b] |= 2;
+            CU(cudaMemcpyAsync(warm_y + row_off[b], y0[b], sizeof(double) * lps[b].num_rows, cudaMemcpyDefault, s));
+        }
+    }
+    if (any_warm) CU(cudaMemcpyAsync(warm, warm_host.data(), sizeof(int) * count, cudaMemcpyHostToDevice, s));
     std::vector<double> host_off(2 * (size_t)count);
     for (int b = 0; b < count; ++b) {
         host_off[b] = lps[b].objective_offset;
@@ -466,6 +488,9 @@ int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o,
     B.offset = offsets;
     B.flags = flags;
     B.nlp = count;
+    B.warm = warm;
+    B.warm_x = warm_x;
+    B.warm_y = warm_y;
     int* active = static_cast<int*>(at(o_active));
     B.active = active;
     B.active_count = active + 2LL * kMaxTiles;

@@ -43,6 +43,9 @@ struct BatchRefs {
     DevState* st;              // [nlp]
     const double* offset;      // [nlp] objective offsets
     int* flags;                // [nlp] setup certificates: 1 crossed bounds, 2 row activity
+    const int* warm;           // [nlp] starting point given: 1 primal, 2 dual (NULL: none)
+    const double* warm_x;      // [n] packed starting primal (original space)
+    const double* warm_y;      // [m] packed starting dual
     TileTable cols, rows;
     const int* active;         // [2 * kMaxTiles] running column tiles, then running row tiles
     const int* active_count;   // [2] lengths of the two lists
@@ -406,7 +409,10 @@ __global__ void kb_setup_cols(const int* __restrict__ col_start, const double* _
         double nrm = 0.0;
         for (int p = col_start[j]; p < col_start[j + 1]; ++p) nrm += fabs(value[p]);
         const_cast<double*>(P.col_norm)[j] = (nrm < 1e-12) ? 1.0 : nrm;
-        const double x0 = clampv(0.0, lsent, hsent);
+        // start as k_setup_cols: the caller's point scaled into the
+        // equilibrated space and projected, else proj(0)
+        const double start = (B.warm && (B.warm[lp] & 1)) ? __dmul_rn(B.warm_x[j], inv) : 0.0;
+        const double x0 = clampv(start, lsent, hsent);
         P.x[j] = x0;
         P.x_avg[j] = x0;
     }
@@ -459,8 +465,9 @@ __global__ void kb_setup_rows(const int* __restrict__ row_start, const int* __re
         const_cast<double*>(P.row_norm)[i] = (nrm < 1e-12) ? 1.0 : nrm;
         const double slack = 1e-9 * (1.0 + mag + maxv(isfinite(l0) ? fabs(l0) : 0.0, isfinite(h0) ? fabs(h0) : 0.0));
         if ((isfinite(l0) && amax < l0 - slack) || (isfinite(h0) && amin > h0 + slack)) infeasible = 1;
-        P.y[i] = 0.0;
-        P.y_avg[i] = 0.0;
+        const double y0 = (B.warm && (B.warm[lp] & 2)) ? __dmul_rn(B.warm_y[i], 1.0 / s) : 0.0;
+        P.y[i] = y0;
+        P.y_avg[i] = y0;
     }
     if (infeasible) atomicOr(B.flags + lp, 2);
     bmax = block_reduce(bmax, scratch, OpMax());

@@ -283,7 +283,16 @@ int mc_pdlp_ctx_solve_batch(mc_pdlp_ctx* c, const mc_lp* lps, int32_t count, con
     Ctx* ctx = reinterpret_cast<Ctx*>(c);
     if (!ctx) return set_error(MC_ERR_INVALID_ARGUMENT, "context is NULL");
     DeviceGuard guard(ctx->device);
-    return solve_batch(*ctx, lps, count, options, primal_out, dual_out, results);
+    return solve_batch(*ctx, lps, count, options, nullptr, nullptr, primal_out, dual_out, results);
+}
+
+int mc_pdlp_ctx_solve_batch_warm(mc_pdlp_ctx* c, const mc_lp* lps, int32_t count, const mc_pdlp_options* options,
+                                 const double* const* initial_primal, const double* const* initial_dual,
+                                 double* const* primal_out, double* const* dual_out, mc_pdlp_result* results) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(c);
+    if (!ctx) return set_error(MC_ERR_INVALID_ARGUMENT, "context is NULL");
+    DeviceGuard guard(ctx->device);
+    return solve_batch(*ctx, lps, count, options, initial_primal, initial_dual, primal_out, dual_out, results);
 }
 
 int mc_pdlp_solve(const mc_lp* lp, const mc_pdlp_options* options, const double* initial_primal,

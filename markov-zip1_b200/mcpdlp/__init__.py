@@ -233,9 +233,12 @@ class Context:
             x, y = np.zeros(0), np.zeros(0)
         return _result_from(res, x, y, trace)
 
-    def solve_batch(self, models: list, options: Optional[PdlpOptions] = None) -> list:
+    def solve_batch(self, models: list, options: Optional[PdlpOptions] = None,
+                    initial_primal: Optional[list] = None, initial_dual: Optional[list] = None) -> list:
         """Solve many independent LPs together (mc_pdlp_ctx_solve_batch): one
-        PdlpResult per model, each from its own run of the algorithm."""
+        PdlpResult per model, each from its own run of the algorithm.  With
+        initial_primal / initial_dual (lists with an array or None per model)
+        each LP starts from its given point (mc_pdlp_ctx_solve_batch_warm)."""
         options = options or PdlpOptions()
         o = options.to_struct()
         count = len(models)
@@ -247,8 +250,28 @@ class Context:
         xp = (C.c_void_p * count)(*[a.ctypes.data if len(a) else None for a in xs])
         yp = (C.c_void_p * count)(*[a.ctypes.data if len(a) else None for a in ys])
         res = (_abi.McPdlpResult * count)()
-        _raise(self._lib.mc_pdlp_ctx_solve_batch(self._h, C.addressof(lps), count, C.addressof(o),
-                                                 C.addressof(xp), C.addressof(yp), C.addressof(res)))
+        if initial_primal is None and initial_dual is None:
+            _raise(self._lib.mc_pdlp_ctx_solve_batch(self._h, C.addressof(lps), count, C.addressof(o),
+                                                     C.addressof(xp), C.addressof(yp), C.addressof(res)))
+        else:
+            keep = []
+
+            def starts(given, sizes):
+                out = (C.c_void_p * count)()
+                for b in range(count):
+                    v = None if given is None else given[b]
+                    if v is not None:
+                        a = np.ascontiguousarray(v, dtype=np.float64)
+                        if a.shape != (sizes[b],):
+                            raise ValueError("starting point dimension mismatch")
+                        keep.append(a)
+                        out[b] = a.ctypes.data
+                return out
+            x0 = starts(initial_primal, [mm.num_cols for mm in models])
+            y0 = starts(initial_dual, [mm.num_rows for mm in models])
+            _raise(self._lib.mc_pdlp_ctx_solve_batch_warm(self._h, C.addressof(lps), count, C.addressof(o),
+                                                          C.addressof(x0), C.addressof(y0), C.addressof(xp),
+                                                          C.addressof(yp), C.addressof(res)))
         return [_result_from(res[b], xs[b], ys[b]) for b in range(count)]
 
     def verify_primal(self, model: Model, primal, claimed_objective: float,

@@ -50,17 +50,21 @@ class NodeLpResult:
 def solve_node_relaxations(ctx: Context, nodes: list, max_iterations: int = 500000,
                            feasibility_tolerance: float = 1e-7,
                            precision: Precision = Precision.fp64,
-                           options: Optional[PdlpOptions] = None) -> list:
+                           options: Optional[PdlpOptions] = None,
+                           warm_primal: Optional[list] = None, warm_dual: Optional[list] = None) -> list:
     """LP relaxations of `nodes` (Models) in one batched solve.  The defaults
     are milp::Options' max_iterations and feasibility_tolerance
     (include/markov_cero/milp/milp_solver.hpp:15-32); the tolerance is the
-    PDLP relative KKT tolerance."""
+    PDLP relative KKT tolerance.  warm_primal / warm_dual (a point or None per
+    node) start each node where its parent ended, as the reference's node
+    solve starts the dual simplex from the parent's basis
+    (src/milp/node_lp.cpp:44-60)."""
     o = options or PdlpOptions()
     o.max_iterations = max_iterations
     o.set_tolerance(feasibility_tolerance)
     o.precision = precision
     out = []
-    for r in ctx.solve_batch(list(nodes), o):
+    for r in ctx.solve_batch(list(nodes), o, initial_primal=warm_primal, initial_dual=warm_dual):
         res = NodeLpResult(status=_FROM_PDLP[r.status], iterations=r.iterations)
         if res.status == "optimal":
             res.primal = r.primal

@@ -151,3 +151,24 @@ def test_work_queue_with_early_finishers(gpu_ctx, oracle):
         assert rel(res[i].objective, cpu.objective) <= 1e-6
     assert res[2].iterations > 10 * res[0].iterations
     assert res[0].iterations == res[3].iterations and res[0].objective == res[3].objective
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32_refine"])
+def test_batch_warm_start_from_solutions(gpu_ctx, precision):
+    """mc_pdlp_ctx_solve_batch_warm: every LP started at its own solution stops
+    at the first check (40 iterations) with the same objective; LPs given no
+    start (None) run from the cold start as in a plain batch."""
+    from mcpdlp import Precision
+    models = generators.batch_part1(9, count=6, m_range=(100, 500))
+    o = opts(1e-8, precision=Precision[precision])
+    cold = gpu_ctx.solve_batch(models, o)
+    xs = [r.primal if b % 3 else None for b, r in enumerate(cold)]
+    ys = [r.dual if b % 3 else None for b, r in enumerate(cold)]
+    warm = gpu_ctx.solve_batch(models, o, initial_primal=xs, initial_dual=ys)
+    for b, (c, w) in enumerate(zip(cold, warm)):
+        assert c.status == w.status == PdlpStatus.optimal
+        if b % 3:
+            assert w.iterations == 40, (b, w.iterations)
+            assert rel(w.objective, c.objective) <= 1e-7
+        else:
+            assert w.iterations == c.iterations and w.objective == c.objective
