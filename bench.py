@@ -20,10 +20,16 @@ relative KKT (the reference's definition).  One step = one full PDLP solve
 * ``cpu_baseline``: the reference's own CPU solve_pdlp (oracle/_ref, built
   from the reference sources) on the same LP, rank 0, one core: setup-only
   and 40-iteration samples, steady iterations/s.
+* ``forms``: the FP32 + FP64-refinement solve of the same LP to 1e-8, and
+  both forms to 1e-4; ``verify_primal_device``: the post-solve check.
 * ``--impl reference``: the reference CPU PDLP alone, same metric and config.
+* ``--workload config2|batch1|batch2``: the precision-stress LP, the 256
+  uneven LPs and the 512 node variants (batched; FP32 + refinement with FP64
+  beside it); ``--ncu-case``: a short profiled solve for ncu captures.
 
 N > 1 (torchrun): a single LP does not shard (replicas only), so every rank
-solves its own replica; no collective touches the data path.
+solves its own replica; no collective touches the data path.  The batch
+workloads shard by LP (nonzero-balanced, weak scaling).
 """
 from __future__ import annotations
 

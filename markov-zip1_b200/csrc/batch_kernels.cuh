@@ -13,10 +13,11 @@
 //
 // Work queue: the iteration kernels are persistent (one wave of resident
 // blocks) and walk a compacted list of the tiles whose LP is still running,
-// block b taking entries b, b + grid, b + 2 grid, ...  kb_compact rebuilds the
-// list after every restart check (the only place an LP terminates), so an LP
-// that has converged costs nothing from its next chunk on, and the long tail
-// where a few slow LPs run on alone costs only their own tiles.
+// block b taking entries b, b + grid, b + 2 grid, ...  kb_compact and
+// kb_fill_active rebuild the list after every restart check (the only place an
+// LP terminates), so an LP that has converged costs nothing from its next
+// chunk on, and the long tail where a few slow LPs run on alone costs only
+// their own tiles.
 //
 // The row and column work inside a tile is the single-LP kernels' (lanes per
 // line, cache policies, fused updates), so the per-nonzero cost is the same.
