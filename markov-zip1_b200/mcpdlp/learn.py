@@ -7,8 +7,8 @@
 
 ``solve_warm`` feeds the network's prediction to the engine with
 ``warm_start_guard`` on: the engine evaluates the reference's KKT score of the
-prediction and of the cold start and runs from the better one, so the plain
-method stays the judge of the error.
+prediction and of the cold start and runs from the better one, so a poor
+prediction never costs more than a cold start.
 
 CLI (training and evaluation on the transportation family):
 

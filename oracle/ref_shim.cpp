@@ -115,7 +115,7 @@ int ref_last_error(char* buf, size_t len) {
     return 0;
 }
 
-// The reference solve, exactly as a library caller runs it (SURVEY call stack B).
+// The reference solve, exactly as a library caller runs it.
 int ref_solve_pdlp(const mc_lp* lp, const mc_pdlp_options* o, double* primal_out,
                    double* dual_out, mc_pdlp_result* r) {
     try {
