@@ -7,8 +7,8 @@
 
 ``solve_warm`` feeds the network's prediction to the engine with
 ``warm_start_guard`` on: the engine evaluates the reference's KKT score of the
-prediction and of the cold start and runs from the better one, so a poor
-prediction never costs more than a cold start.
+prediction and of the cold start and runs from the better-scoring point, and
+PDHG runs to the same tolerance either way.
 
 CLI (training and evaluation on the transportation family):
 
