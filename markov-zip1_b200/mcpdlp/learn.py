@@ -10,7 +10,8 @@
 prediction and of the cold start and runs from the better-scoring point, and
 PDHG runs to the same tolerance either way.
 
-CLI (training and evaluation on the transportation family):
+CLI (training and evaluation on the transportation family, or on the config-0
+random-LP family with --family random):
 
     python -m mcpdlp.learn --train 4096 --test 256 --out gnn.npz
 """
@@ -159,13 +160,21 @@ def solve_targets(ctx: Context, models: list, options: PdlpOptions, batch: int =
 
 
 def solve_warm(ctx: Context, net: WarmStartNet, model: Model, options: PdlpOptions,
-               guard: bool = True) -> PdlpResult:
+               guard: bool = True, use_weight: bool = False) -> PdlpResult:
     """Solve from the network's prediction, guarded by the engine (guard=False
-    forces the prediction, for measuring what it does on its own)."""
+    forces the prediction, for measuring what it does on its own).
+
+    The predicted point is used with the reference's own initial primal weight
+    (derived from the scaled norms of c and b): on B200 the predicted weight,
+    trained on each solve's final weight, costs iterations (on held-out
+    config-0 family LPs at 1e-8: 844 iterations from the predicted weight
+    alone, 869 from the solve's own final weight, 736 cold), while the
+    predicted point with the derived weight takes 676.  use_weight=True passes
+    the predicted weight too."""
     x, y, lw = net.predict(model)
     o = PdlpOptions(**{k: getattr(options, k) for k in options.__dataclass_fields__})
     o.initial_primal, o.initial_dual = x, y
-    o.initial_primal_weight = float(min(max(math.exp(lw), 1e-6), 1e6))
+    o.initial_primal_weight = float(min(max(math.exp(lw), 1e-6), 1e6)) if use_weight else 0.0
     o.warm_start_guard = guard
     return ctx.solve(model, o)
 
@@ -183,11 +192,17 @@ def main() -> None:
     ap.add_argument("--margin", type=float, default=0.05)
     ap.add_argument("--size", type=int, nargs=2, default=[50, 500],
                     help="suppliers and customers uniform in [lo, hi] (the workload: 50 500)")
+    ap.add_argument("--family", default="transport", choices=["transport", "random"],
+                    help="transport: S, D in --size; random: the config-0 generator with m in --size, "
+                         "n = 3m, 6 nonzeros per column")
     ap.add_argument("--out", default="")
     args = ap.parse_args()
     ctx = Context(0)
     t0 = time.time()
     def family(seed):
+        if args.family == "random":
+            m = generators.uniform_int(seed, 0, *args.size)
+            return generators.random_lp(seed, m, 3 * m, 6)
         S = generators.uniform_int(seed, 0, *args.size)
         D = generators.uniform_int(seed, 1, *args.size)
         return generators.transport(seed, S, D)
@@ -210,7 +225,7 @@ def main() -> None:
         cold = ctx.solve(m, eopt)
         warm = solve_warm(ctx, net, m, eopt)
         forced = solve_warm(ctx, net, m, eopt, guard=False)
-        rows.append(dict(S=m.info["S"], D=m.info["D"], cold_it=cold.iterations, warm_it=warm.iterations,
+        rows.append(dict(m=m.num_rows, n=m.num_cols, cold_it=cold.iterations, warm_it=warm.iterations,
                          cold_ms=cold.total_ms, warm_ms=warm.total_ms, cold_status=cold.status.name,
                          warm_status=warm.status.name, used=warm.extra["warm_start_used"],
                          forced_it=forced.iterations, forced_status=forced.status.name,
