@@ -260,9 +260,10 @@ int mc_pdlp_ctx_solve_batch_warm(mc_pdlp_ctx* ctx, const mc_lp* lps, int32_t cou
  * `rounds` rounds, FP32) that predicts a primal/dual starting point and the
  * log of the initial primal weight.  Trained and run on the GPU by the
  * engine's own forward/backward kernels.  LPs are read from host memory.
- * Feed the prediction to mc_pdlp_ctx_solve as initial_primal / initial_dual /
- * initial_primal_weight with warm_start_guard = 1, which falls back to the
- * cold start whenever the prediction's KKT score is worse.
+ * Feed the prediction to mc_pdlp_ctx_solve as initial_primal / initial_dual
+ * with warm_start_guard = 1, which falls back to the cold start whenever the
+ * prediction's KKT score is worse.  Leave initial_primal_weight at 0 (the
+ * derived weight): the predicted weight cost iterations in measurement.
  */
 typedef struct mc_gnn mc_gnn;
 int mc_gnn_create(int device, int rounds, uint64_t seed, mc_gnn** out);
