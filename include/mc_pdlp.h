@@ -390,8 +390,9 @@ int mc_lp_file_read(const char* path, mc_lp* lp);
 /*
  * mc_ruiz_equilibrate_noalloc: the same equilibration as mc_ruiz_equilibrate,
  * with bit-identical results, for callers that cannot allocate device memory
- * (work inside CUDA stream capture, device memory owned by another allocator,
- * a request path that must not allocate).  No counterpart in the reference.
+ * (device memory all owned by another allocator such as a caching pool or a
+ * fixed arena; a request path that must not allocate, since an allocation can
+ * wait on the device for an unbounded time).  No counterpart in the reference.
  * It allocates nothing: its working memory is one static device array of
  * about 8 MiB that every GPU loading the library holds until exit.
  * Limits: m + n <= 1,048,576, else MC_ERR_RESOURCE_LIMIT (nothing launched).

@@ -1,10 +1,10 @@
 // Ruiz equilibration with no device allocation: mc_ruiz_equilibrate_noalloc.
 //
-// Some callers cannot call cudaMalloc: a solver that runs the equilibration
-// inside CUDA stream capture (allocation is not a capturable operation), an
-// application whose device memory is entirely owned by another allocator (a
-// framework's caching pool, a fixed arena sized at start-up), or a service
-// that must not allocate on its request path.  This entry point does the same
+// Some callers cannot call cudaMalloc: an application whose device memory is
+// entirely owned by another allocator (a framework's caching pool, a fixed
+// arena sized at start-up), where a stray cudaMalloc can fail or fragment the
+// pool, or a service that must not allocate on its request path, because an
+// allocation can wait on the device and its latency has no bound.  This entry point does the same
 // work as mc_ruiz_equilibrate, with the same arithmetic and bit-identical
 // results, but every byte of working memory it needs beyond the caller's
 // inputs and outputs lives in one file-scope device array, g_ruiz_scratch,

@@ -1,8 +1,9 @@
 """Ruiz equilibration for callers that cannot allocate device memory.
 
-mc_ruiz_equilibrate_noalloc serves code that must not call cudaMalloc: work
-recorded inside CUDA stream capture, applications whose device memory is all
-owned by another allocator, request paths that may not allocate.  It keeps its
+mc_ruiz_equilibrate_noalloc serves code that must not call cudaMalloc:
+applications whose device memory is all owned by another allocator (a caching
+pool, a fixed arena), and request paths that may not allocate because an
+allocation can wait on the device for an unbounded time.  It keeps its
 working memory in one static device array instead.  These tests call it
 through the C ABI, twice and three times in a row on the same array, and
 compare every output with the allocating entry point mc_ruiz_equilibrate.
