@@ -106,3 +106,27 @@ def test_invalid_inputs_are_errors(gpu_ctx):
         gpu_ctx.verify_primal(m, np.zeros(m.num_cols), float("inf"))
     # the context stays usable
     assert gpu_ctx.verify_primal(m, np.zeros(m.num_cols), 0.0, 1e-4, 1e-4)["violations"]["row_lower"] >= 0
+
+
+def test_empty_rows_and_empty_models(gpu_ctx, reference):
+    """Rows without entries have activity 0 and are still checked against
+    their bounds; a model without rows or without nonzeros verifies its
+    variable bounds and objective only -- as the reference does."""
+    inf = np.inf
+    # row 1 has no entries and bounds [1, 2]: activity 0 violates its lower bound
+    m = mcpdlp.from_triplets(3, 2, [0, 2], [0, 1], [1.0, 2.0], objective=[1.0, -1.0],
+                             var_lower=[0.0, 0.0], var_upper=[4.0, inf], row_lower=[0.0, 1.0, -inf],
+                             row_upper=[3.0, 2.0, 5.0])
+    for x, claimed in (([1.0, 1.0], 0.0), ([5.0, 3.0], 2.0), ([0.5, 0.25], 0.25)):
+        x = np.array(x)
+        check_same(gpu_ctx.verify_primal(m, x, claimed, 1e-7, 1e-7),
+                   reference.verify_report(m, x, claimed, 1e-7, 1e-7))
+    no_rows = mcpdlp.Model(0, 2, np.zeros(3, np.int32), np.zeros(0, np.int32), np.zeros(0),
+                           np.array([1.0, 2.0]), np.zeros(2), np.ones(2), np.zeros(0), np.zeros(0))
+    no_nnz = mcpdlp.Model(2, 2, np.zeros(3, np.int32), np.zeros(0, np.int32), np.zeros(0),
+                          np.array([1.0, 2.0]), np.zeros(2), np.ones(2), np.array([-1.0, 0.5]),
+                          np.array([1.0, 1.0]))
+    for mm in (no_rows, no_nnz):
+        for x in (np.array([0.5, 0.5]), np.array([2.0, -1.0])):
+            check_same(gpu_ctx.verify_primal(mm, x, 1.5, 1e-7, 1e-7),
+                       reference.verify_report(mm, x, 1.5, 1e-7, 1e-7))

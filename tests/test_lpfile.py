@@ -19,7 +19,7 @@ def same(a, b) -> None:
     assert a.objective_offset == b.objective_offset and int(a.objective_sense) == int(b.objective_sense)
 
 
-@pytest.mark.parametrize("which", ["netlib_afiro", "tiny_simplex", "random", "maximise", "empty_rows"])
+@pytest.mark.parametrize("which", ["netlib_afiro", "tiny_simplex", "random", "maximise", "empty_rows", "no_rows"])
 def test_host_round_trip(tmp_path, which):
     if which == "random":
         m = generators.random_lp(3, 300, 900, 6, "precision")   # infinite upper bounds
@@ -29,6 +29,9 @@ def test_host_round_trip(tmp_path, which):
     elif which == "empty_rows":
         m = mcpdlp.Model(3, 2, np.array([0, 1, 1], np.int32), np.array([2], np.int32), np.array([1.5]),
                          np.ones(2), np.zeros(2), np.full(2, np.inf), np.full(3, -np.inf), np.ones(3))
+    elif which == "no_rows":
+        m = mcpdlp.Model(0, 2, np.zeros(3, np.int32), np.zeros(0, np.int32), np.zeros(0), np.ones(2),
+                         np.zeros(2), np.ones(2), np.zeros(0), np.zeros(0))
     else:
         m = load_model(which)
     path = tmp_path / f"{which}.mclp"
