@@ -172,3 +172,24 @@ def test_batch_warm_start_from_solutions(gpu_ctx, precision):
             assert rel(w.objective, c.objective) <= 1e-7
         else:
             assert w.iterations == c.iterations and w.objective == c.objective
+
+
+def test_batch_maximize_and_offset_members(gpu_ctx, oracle):
+    """Per-LP objective sense and offset in one batch: each member follows its
+    own solve (a maximisation LP stops at the iteration limit, as the reference
+    does: its gap mixes the maximisation objective with a minimisation-sign
+    dual objective, src/lp/first_order/pdlp.cpp:113-131)."""
+    mx = generators.random_lp(31, 120, 360, 5)
+    mx.objective_sense, mx.objective_offset = 1, 7.5
+    mn = generators.random_lp(32, 150, 450, 5)
+    mn.objective_offset = -2.25
+    o = opts(1e-8, max_iterations=2000)
+    res = gpu_ctx.solve_batch([mx, mn], o)
+    for model, r in zip((mx, mn), res):
+        single = gpu_ctx.solve(model, o)
+        cpu = oracle.solve(model, options(1e-8, max_iterations=2000))
+        assert r.status == single.status == cpu.status
+        assert rel(r.objective, cpu.objective) <= 1e-6
+    assert res[0].status == PdlpStatus.iteration_limit
+    assert res[1].status == PdlpStatus.optimal
+    assert rel(res[1].objective, mn.info["optimum"] + mn.objective_offset) <= 1e-6
