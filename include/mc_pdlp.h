@@ -105,9 +105,6 @@ typedef struct mc_pdlp_options {
     int32_t device;                   /* CUDA ordinal used by mc_pdlp_solve, default 0 */
     int32_t profile_kernels;          /* 1: time every kernel launch with CUDA events
                                          (no CUDA graph; slower); fills kernel_ms_by_kind */
-    int32_t refine_max_rounds;        /* unused (default 12): FP32_REFINE refines at every
-                                         restart, see refinement_rounds in the result */
-    double refine_inner_tolerance;    /* unused (default 1e-4), as refine_max_rounds */
     int32_t check_every_chunks;       /* host status poll interval in restart chunks, default 1 */
     int32_t lanes_per_column;         /* A^T y kernel: 0 = automatic (single LP: by mean
                                          column length; batch: the lanes autotuner, timed on
@@ -218,6 +215,43 @@ int mc_pdlp_ctx_solve(mc_pdlp_ctx* ctx, const mc_lp* lp, const mc_pdlp_options* 
                       const double* initial_primal, const double* initial_dual,
                       double* primal_out, double* dual_out,
                       mc_pdlp_result* result, mc_pdlp_trace* trace);
+
+/* The context's CUDA stream (a cudaStream_t), on which every kernel of the
+ * context runs: callers time the engine with CUDA events recorded on it. */
+int mc_pdlp_ctx_stream(mc_pdlp_ctx* ctx, void** stream);
+
+/*
+ * Stepwise form of mc_pdlp_ctx_solve: the same solve driven a few restart
+ * chunks at a time, so that a caller can time, interleave or stop the PDHG
+ * loop (pdlp.cpp:194-262) between chunks.  The reference's solve_pdlp runs
+ * the loop in one call; begin + iterate (to the end) + finish gives the same
+ * result as mc_pdlp_ctx_solve, bit for bit.
+ *   mc_pdlp_ctx_begin:   everything before the first iteration (uploads,
+ *                        validation, transpose, Ruiz, norms, start point,
+ *                        pdlp.cpp:139-191); arguments as mc_pdlp_ctx_solve.
+ *                        Host arrays of `lp` are copied during the call; device
+ *                        arrays (and `trace`) must stay valid until finish.
+ *   mc_pdlp_ctx_iterate: up to `chunks` further chunks (each restart_every
+ *                        iterations and the restart check); returns with the
+ *                        context's stream synchronised.  *iterations (may be
+ *                        NULL): iterations done so far; *finished (may be
+ *                        NULL): 1 once the solve has converged, failed or
+ *                        reached max_iterations' last whole chunk.
+ *   mc_pdlp_ctx_finish:  the remaining partial chunk and final evaluation if
+ *                        the loop reached max_iterations (pdlp.cpp:263-265),
+ *                        then outputs and result as mc_pdlp_ctx_solve.  A solve
+ *                        finished early reports iteration_limit with the last
+ *                        check's averages, as a solve with max_iterations set
+ *                        to the iterations done would.
+ * One solve in progress per context: any other solve, batch or verify call on
+ * the context ends it (iterate / finish then return MC_ERR_INVALID_ARGUMENT).
+ */
+int mc_pdlp_ctx_begin(mc_pdlp_ctx* ctx, const mc_lp* lp, const mc_pdlp_options* options,
+                      const double* initial_primal, const double* initial_dual,
+                      mc_pdlp_trace* trace);
+int mc_pdlp_ctx_iterate(mc_pdlp_ctx* ctx, int64_t chunks, int64_t* iterations, int32_t* finished);
+int mc_pdlp_ctx_finish(mc_pdlp_ctx* ctx, double* primal_out, double* dual_out,
+                       mc_pdlp_result* result);
 
 /* One-shot form: a temporary context on options->device. */
 int mc_pdlp_solve(const mc_lp* lp, const mc_pdlp_options* options,

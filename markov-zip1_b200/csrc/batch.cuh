@@ -282,6 +282,7 @@ static void make_tiles(const std::vector<long long>& off, int per_tile, std::vec
 
 int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o, const double* const* x0,
                 const double* const* y0, double* const* x_out, double* const* y_out, mc_pdlp_result* results) {
+    ctx.drop_session();  // the batch reuses the arena
     const double t_begin = now_ms();
     if (!lps || count <= 0 || !results) return set_error(MC_ERR_INVALID_ARGUMENT, "empty batch");
     TRY(validate_options(o));

@@ -105,6 +105,24 @@ __device__ __forceinline__ void st_keep(float* a, float v, unsigned long long po
 }
 template <class T>
 __device__ __forceinline__ T ld_stream(const T* a) { return __ldcs(a); }
+// 16-byte streaming loads of four indices / two doubles / four floats (the
+// address must be 16-byte aligned)
+__device__ __forceinline__ int4 ld_stream4(const int* a) { return __ldcs(reinterpret_cast<const int4*>(a)); }
+__device__ __forceinline__ void ld_stream_quad(const double* a, double& v0, double& v1, double& v2, double& v3) {
+    const double2 lo = __ldcs(reinterpret_cast<const double2*>(a));
+    const double2 hi = __ldcs(reinterpret_cast<const double2*>(a + 2));
+    v0 = lo.x;
+    v1 = lo.y;
+    v2 = hi.x;
+    v3 = hi.y;
+}
+__device__ __forceinline__ void ld_stream_quad(const float* a, float& v0, float& v1, float& v2, float& v3) {
+    const float4 q = __ldcs(reinterpret_cast<const float4*>(a));
+    v0 = q.x;
+    v1 = q.y;
+    v2 = q.z;
+    v3 = q.w;
+}
 template <class T>
 __device__ __forceinline__ void st_stream(T* a, T v) { __stcs(a, v); }
 

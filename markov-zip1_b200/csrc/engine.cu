@@ -93,6 +93,7 @@ int Arena::reserve(size_t bytes) {
 // ------------------------------------------------------------------ context
 Ctx::~Ctx() {
     if (device >= 0) cudaSetDevice(device);
+    drop_session();
     release_graphs();
     if (arena.base) cudaFree(arena.base);
     if (h_state) cudaFreeHost(h_state);
@@ -215,8 +216,6 @@ void mc_pdlp_default_options(mc_pdlp_options* o) {
     o->precision = MC_PRECISION_FP64;
     o->device = 0;
     o->profile_kernels = 0;
-    o->refine_max_rounds = 12;
-    o->refine_inner_tolerance = 1e-4;
     o->check_every_chunks = 1;
 }
 
@@ -276,6 +275,48 @@ int mc_pdlp_ctx_solve(mc_pdlp_ctx* c, const mc_lp* lp, const mc_pdlp_options* op
     DeviceGuard guard(ctx->device);
     return solve_lp(*ctx, lp, options, initial_primal, initial_dual, primal_out, dual_out, result,
                     trace);
+}
+
+int mc_pdlp_ctx_stream(mc_pdlp_ctx* c, void** stream) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(c);
+    if (!ctx || !stream) return set_error(MC_ERR_INVALID_ARGUMENT, "context or stream is NULL");
+    *stream = reinterpret_cast<void*>(ctx->stream);
+    return MC_OK;
+}
+
+int mc_pdlp_ctx_begin(mc_pdlp_ctx* c, const mc_lp* lp, const mc_pdlp_options* options,
+                      const double* initial_primal, const double* initial_dual, mc_pdlp_trace* trace) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(c);
+    if (!ctx) return set_error(MC_ERR_INVALID_ARGUMENT, "context is NULL");
+    DeviceGuard guard(ctx->device);
+    const int rc = begin_session(*ctx, lp, options, initial_primal, initial_dual, trace);
+    if (rc != MC_OK) ctx->drop_session();
+    return rc;
+}
+
+int mc_pdlp_ctx_iterate(mc_pdlp_ctx* c, int64_t chunks, int64_t* iterations, int32_t* finished) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(c);
+    if (!ctx) return set_error(MC_ERR_INVALID_ARGUMENT, "context is NULL");
+    DeviceGuard guard(ctx->device);
+    long long it = 0;
+    int fin = 0;
+    const int rc = iterate_session(*ctx, (long long)chunks, &it, &fin);
+    if (rc != MC_OK) {
+        ctx->drop_session();
+        return rc;
+    }
+    if (iterations) *iterations = it;
+    if (finished) *finished = fin;
+    return MC_OK;
+}
+
+int mc_pdlp_ctx_finish(mc_pdlp_ctx* c, double* primal_out, double* dual_out, mc_pdlp_result* result) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(c);
+    if (!ctx) return set_error(MC_ERR_INVALID_ARGUMENT, "context is NULL");
+    DeviceGuard guard(ctx->device);
+    const int rc = finish_session(*ctx, primal_out, dual_out, result);
+    if (rc != MC_OK) ctx->drop_session();
+    return rc;
 }
 
 int mc_pdlp_ctx_solve_batch(mc_pdlp_ctx* c, const mc_lp* lps, int32_t count, const mc_pdlp_options* options,

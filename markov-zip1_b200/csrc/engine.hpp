@@ -66,6 +66,9 @@ struct Layout {
     }
 };
 
+struct Session;                 // a stepwise solve in progress (solve.cuh)
+void free_session(Session* s);
+
 struct Ctx {
     int device = -1;
     int sm_count = 0;
@@ -91,8 +94,15 @@ struct Ctx {
     std::vector<cudaEvent_t> prof_events;
     size_t prof_used = 0;
 
+    // the stepwise solve in progress; any other use of the arena ends it
+    Session* session = nullptr;
+
     ~Ctx();
     int init(int device);
+    void drop_session() {
+        free_session(session);
+        session = nullptr;
+    }
     void release_graphs();
     void begin_launch(int kind);
     void end_launch();
@@ -130,5 +140,9 @@ int pick_lanes(double mean_len);
 int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* warm_x,
              const double* warm_y, double* x_out, double* y_out, mc_pdlp_result* res,
              mc_pdlp_trace* trace);
+int begin_session(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* warm_x,
+                  const double* warm_y, mc_pdlp_trace* trace);
+int iterate_session(Ctx& ctx, long long chunks, long long* iterations, int* finished);
+int finish_session(Ctx& ctx, double* x_out, double* y_out, mc_pdlp_result* res);
 
 }  // namespace mc

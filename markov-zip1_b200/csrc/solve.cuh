@@ -7,8 +7,10 @@
 #include "staged.cuh"
 #include "mixed.cuh"
 
+#include <climits>
 #include <cmath>
 #include <cstring>
+#include <new>
 
 namespace mc {
 
@@ -399,71 +401,97 @@ int chunk_graph(Ctx& ctx, const E& eng, long long base, long long R, const Contr
     return MC_OK;
 }
 
-// The PDHG loop (pdlp.cpp:194-275) in restart chunks, each a CUDA graph
-// replay; the host polls the device state one chunk group behind.  Returns
-// with the stream synchronised.
-template <class E>
-int run_chunks(Ctx& ctx, const E& eng, DevState* st, long long maxit, long long R, int poll_every,
-               const Controls& ctl, const TraceBuf& tr) {
-    cudaStream_t s = ctx.stream;
-    ctx.release_graphs();
-    const long long full_chunks = maxit / R;
-    long long base = 0;
-    bool done = false;
+// Progress of the PDHG loop (pdlp.cpp:194-275) over restart chunks; kept
+// between calls so that a solve can be driven a few chunks at a time.
+struct ChunkLoop {
+    long long full_chunks = 0;  // whole chunks within max_iterations
+    long long chunk = 0;        // chunks enqueued so far
+    long long base = 0;         // global iteration at the start of the next chunk
+    bool done = false;          // a terminal status was seen by a poll
+    bool have_prev = false;     // a poll is in flight
+    int inflight = 0, ev_idx = 0;
+    int cls = 0;                // the engine's launch-shape class, from the last poll
     long long recipe[40][MC_KERNEL_KINDS] = {};
-    int inflight = 0;
-    int ev_idx = 0;
-    bool have_prev = false;
-    int cls = 0;  // the engine's launch-shape class, from the last poll
-    for (long long chunk = 0; chunk < full_chunks && !done; ++chunk) {
-        eng.use_class(cls);
+};
+
+// Enqueue up to `max_chunks` further chunks (each a CUDA graph replay), the
+// host polling the device state one chunk group behind, so that the GPU never
+// idles between chunks.  Returns with the stream synchronised and the state
+// of the last chunk in ctx.h_state[2].
+template <class E>
+int loop_chunks(Ctx& ctx, const E& eng, DevState* st, ChunkLoop& L, long long max_chunks, long long R,
+                int poll_every, const Controls& ctl, const TraceBuf& tr) {
+    cudaStream_t s = ctx.stream;
+    const long long stop = L.chunk + std::min(max_chunks, L.full_chunks - L.chunk);
+    for (; L.chunk < stop && !L.done; ++L.chunk) {
+        eng.use_class(L.cls);
         if (ctx.profiling) {
-            TRY(enqueue_span(ctx, eng, base, 0, (int)R, ctl));
+            TRY(enqueue_span(ctx, eng, L.base, 0, (int)R, ctl));
             TRY(eng.check(ctx, R, 0, ctl, tr));
             TRY(ctx.drain_profile());
         } else {
             // graphs keyed by the step-size phase (base % 10) and the class
-            const int key = (int)(base % 10) + 10 * cls;
+            const int key = (int)(L.base % 10) + 10 * L.cls;
             auto it = ctx.graphs.find(key);
             cudaGraphExec_t exec = nullptr;
             if (it == ctx.graphs.end()) {
-                TRY(chunk_graph(ctx, eng, base, R, ctl, tr, key, &exec, recipe[key]));
+                TRY(chunk_graph(ctx, eng, L.base, R, ctl, tr, key, &exec, L.recipe[key]));
             } else {
                 exec = it->second;
             }
             CU(cudaGraphLaunch(exec, s));
-            for (int q = 0; q < MC_KERNEL_KINDS; ++q) ctx.launches[q] += recipe[key][q];
+            for (int q = 0; q < MC_KERNEL_KINDS; ++q) ctx.launches[q] += L.recipe[key][q];
         }
-        base += R;
-        ++inflight;
-        if (inflight >= poll_every || chunk + 1 == full_chunks) {
-            if (have_prev) {
-                CU(cudaEventSynchronize(ctx.ev_poll[ev_idx ^ 1]));
-                if (ctx.h_state[ev_idx ^ 1].done) done = true;
-                cls = eng.shape_class(ctx.h_state[ev_idx ^ 1]);
+        L.base += R;
+        ++L.inflight;
+        if (L.inflight >= poll_every || L.chunk + 1 == stop) {
+            if (L.have_prev) {
+                CU(cudaEventSynchronize(ctx.ev_poll[L.ev_idx ^ 1]));
+                if (ctx.h_state[L.ev_idx ^ 1].done) L.done = true;
+                L.cls = eng.shape_class(ctx.h_state[L.ev_idx ^ 1]);
             }
-            CU(cudaMemcpyAsync(&ctx.h_state[ev_idx], st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
-            CU(cudaEventRecord(ctx.ev_poll[ev_idx], s));
-            have_prev = true;
-            ev_idx ^= 1;
-            inflight = 0;
+            CU(cudaMemcpyAsync(&ctx.h_state[L.ev_idx], st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
+            CU(cudaEventRecord(ctx.ev_poll[L.ev_idx], s));
+            L.have_prev = true;
+            L.ev_idx ^= 1;
+            L.inflight = 0;
         }
     }
     CU(cudaStreamSynchronize(s));
     CU(cudaMemcpy(&ctx.h_state[2], st, sizeof(DevState), cudaMemcpyDeviceToHost));
-    if (!ctx.h_state[2].done) {
-        // the loop ran out: remaining partial chunk, then the final evaluation
-        // (pdlp.cpp:263-265); after a whole number of chunks the last check
-        // already holds the averages' residuals
-        const long long rem = maxit - full_chunks * R;
-        if (rem > 0 || full_chunks == 0) {
-            TRY(enqueue_span(ctx, eng, base, 0, (int)rem, ctl));
+    L.have_prev = false;  // everything enqueued has completed
+    L.inflight = 0;
+    if (ctx.h_state[2].done) L.done = true;
+    return MC_OK;
+}
+
+// After the last whole chunk: the remaining partial chunk, then the final
+// evaluation (pdlp.cpp:263-265); after a whole number of chunks the last
+// check already holds the averages' residuals.
+template <class E>
+int finish_chunks(Ctx& ctx, const E& eng, const ChunkLoop& L, long long maxit, long long R, const Controls& ctl,
+                  const TraceBuf& tr) {
+    if (!L.done && L.chunk == L.full_chunks) {
+        const long long rem = maxit - L.full_chunks * R;
+        if (rem > 0 || L.full_chunks == 0) {
+            TRY(enqueue_span(ctx, eng, L.base, 0, (int)rem, ctl));
             TRY(eng.check(ctx, rem, 1, ctl, tr));
             TRY(ctx.drain_profile());
         }
     }
-    CU(cudaStreamSynchronize(s));
+    CU(cudaStreamSynchronize(ctx.stream));
     return MC_OK;
+}
+
+// The whole PDHG loop (pdlp.cpp:194-275); returns with the stream synchronised.
+template <class E>
+int run_chunks(Ctx& ctx, const E& eng, DevState* st, long long maxit, long long R, int poll_every,
+               const Controls& ctl, const TraceBuf& tr) {
+    ctx.release_graphs();
+    ChunkLoop L;
+    L.full_chunks = maxit / R;
+    TRY(loop_chunks(ctx, eng, st, L, L.full_chunks, R, poll_every, ctl, tr));
+    return finish_chunks(ctx, eng, L, maxit, R, ctl, tr);
 }
 
 // Start selection.  `start(warm)` writes the starting point and resets the
@@ -547,27 +575,65 @@ int validate_lp(const mc_lp* lp) {
     return MC_OK;
 }
 
-int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* warm_x,
-             const double* warm_y, double* x_out, double* y_out, mc_pdlp_result* res,
-             mc_pdlp_trace* trace) {
+// A solve in progress: what the PDHG loop and the output stage need between
+// the calls of a stepwise solve (mc_pdlp_ctx_begin / _iterate / _finish).
+struct Session {
+    bool trivial = false, mixed = false, dev_in = false;
+    Engine64 e64{};
+    EngineMixed emx{};
+    DevState* st = nullptr;
+    Controls ctl{};
+    TraceBuf tr{};
+    mc_pdlp_trace* trace = nullptr;
+    mc_pdlp_options o{};
+    int m = 0, n = 0, poll_every = 1;
+    ChunkLoop loop;
+    double* x = nullptr;  // FP64 iterate (the mixed form's base point)
+    double* y = nullptr;
+    double* x_avg = nullptr;
+    double* y_avg = nullptr;
+    float* fx_avg = nullptr;  // mixed form: averaged corrections
+    float* fy_avg = nullptr;
+    double* col_scale = nullptr;
+    double* row_scale = nullptr;
+    double* x_stage = nullptr;
+    double* y_stage = nullptr;
+    double t_begin = 0.0;
+    mc_pdlp_result head{};  // warm-start fields set at the start
+};
+
+void free_session(Session* s) { delete s; }
+
+// Everything of a solve up to the first iteration (pdlp.cpp:139-191):
+// uploads, validation, transpose, Ruiz, norms, start point.  The session is
+// kept in the context until finish_session() or the next solve.
+int begin_session(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* warm_x,
+                  const double* warm_y, mc_pdlp_trace* trace) {
+    ctx.drop_session();
     const double t_begin = now_ms();
-    if (!res) return set_error(MC_ERR_INVALID_ARGUMENT, "result is NULL");
-    std::memset(res, 0, sizeof *res);
-    std::snprintf(res->backend_actually_used, sizeof res->backend_actually_used, "cuda");
     if (trace) trace->count = 0;
     TRY(validate_options(o));
     TRY(validate_lp(lp));
+    Session* S_ = new (std::nothrow) Session();
+    if (!S_) return set_error(MC_ERR_OUT_OF_MEMORY, "host allocation failed");
+    ctx.session = S_;
+    Session& SS = *S_;
+    SS.t_begin = t_begin;
+    SS.o = *o;
+    SS.trace = trace;
+    mc_pdlp_result* res = &SS.head;
     const int m = lp->num_rows, n = lp->num_cols;
     const long long nnz = lp->nnz;
+    SS.m = m;
+    SS.n = n;
     if (m == 0 || n == 0) {  // pdlp.cpp:144-149
-        res->status = MC_PDLP_OPTIMAL;
-        res->tolerance = o->primal_tolerance;
-        fill_message(res, "trivial");
-        res->total_ms = now_ms() - t_begin;
+        SS.trivial = true;
         return MC_OK;
     }
     const bool mixed = o->precision == MC_PRECISION_FP32_REFINE;
     const bool dev_in = lp->memory == MC_MEMORY_DEVICE;
+    SS.mixed = mixed;
+    SS.dev_in = dev_in;
     cudaStream_t s = ctx.stream;
     for (int q = 0; q < MC_KERNEL_KINDS; ++q) {
         ctx.launches[q] = 0;
@@ -746,11 +812,11 @@ int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* 
                 static_cast<int*>(at(o_tr_rs))};
     const int poll_every = o->check_every_chunks > 0 ? o->check_every_chunks : 1;
 
-    // ---- the PDHG loop
+    // ---- the PDHG engine of the chosen form
     float* fx_avg = nullptr;
     float* fy_avg = nullptr;
     if (!mixed) {
-        Engine64 eng;
+        Engine64& eng = SS.e64;
         Iterates<double>& P = eng.P;
         P.m = m;
         P.n = n;
@@ -783,9 +849,8 @@ int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* 
         TRY(build_tiles(ctx, eng.pl, m, n, csc_start, csr_start, static_cast<int*>(at(o_col_bounds)),
                         static_cast<int*>(at(o_row_bounds)), chunk));
         TRY(choose_start(ctx, eng, st, ctl, have_warm, o->warm_start_guard != 0, start, [] { return MC_OK; }, res));
-        TRY(run_chunks(ctx, eng, st, o->max_iterations, o->restart_every, poll_every, ctl, tr));
     } else {
-        EngineMixed eng;
+        EngineMixed& eng = SS.emx;
         float* f_cscv = static_cast<float*>(at(o_f_cscv));
         float* f_csrv = static_cast<float*>(at(o_f_csrv));
         float* f_g = static_cast<float*>(at(o_fn[0]));
@@ -883,70 +948,135 @@ int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* 
             return eng.recenter(ctx, 1);
         };
         TRY(choose_start(ctx, eng, st, ctl, have_warm, o->warm_start_guard != 0, start, init, res));
-        TRY(run_chunks(ctx, eng, st, o->max_iterations, o->restart_every, poll_every, ctl, tr));
     }
+    SS.st = st;
+    SS.ctl = ctl;
+    SS.tr = tr;
+    SS.poll_every = poll_every;
+    SS.loop.full_chunks = o->max_iterations / o->restart_every;
+    SS.x = x;
+    SS.y = y;
+    SS.x_avg = x_avg;
+    SS.y_avg = y_avg;
+    SS.fx_avg = fx_avg;
+    SS.fy_avg = fy_avg;
+    SS.col_scale = col_scale;
+    SS.row_scale = row_scale;
+    SS.x_stage = x_stage;
+    SS.y_stage = y_stage;
+    ctx.release_graphs();
+    return MC_OK;
+}
+
+// Up to `chunks` further restart chunks of the session's PDHG loop (each
+// restart_every iterations and the restart check, pdlp.cpp:194-262).
+int iterate_session(Ctx& ctx, long long chunks, long long* iterations, int* finished) {
+    Session* S = ctx.session;
+    if (!S) return set_error(MC_ERR_INVALID_ARGUMENT, "no solve in progress on this context");
+    if (chunks < 0) return set_error(MC_ERR_INVALID_ARGUMENT, "chunks must be >= 0");
+    if (!S->trivial && chunks > 0) {
+        const long long R = S->o.restart_every;
+        if (S->mixed) TRY(loop_chunks(ctx, S->emx, S->st, S->loop, chunks, R, S->poll_every, S->ctl, S->tr));
+        else TRY(loop_chunks(ctx, S->e64, S->st, S->loop, chunks, R, S->poll_every, S->ctl, S->tr));
+    }
+    if (iterations) *iterations = S->trivial ? 0 : S->loop.chunk * S->o.restart_every;
+    if (finished) *finished = (S->trivial || S->loop.done || S->loop.chunk == S->loop.full_chunks) ? 1 : 0;
+    if (S->loop.done && iterations && !S->trivial) *iterations = ctx.h_state[2].iter;
+    return MC_OK;
+}
+
+// The end of a solve: the remaining partial chunk and final evaluation when
+// the loop ran to max_iterations, then the unscaled averages (pdlp.cpp:263-276)
+// and the result.  Ends the session.
+int finish_session(Ctx& ctx, double* x_out, double* y_out, mc_pdlp_result* res) {
+    Session* S = ctx.session;
+    if (!S) return set_error(MC_ERR_INVALID_ARGUMENT, "no solve in progress on this context");
+    if (!res) return set_error(MC_ERR_INVALID_ARGUMENT, "result is NULL");
+    std::memcpy(res, &S->head, sizeof *res);
+    std::snprintf(res->backend_actually_used, sizeof res->backend_actually_used, "cuda");
+    const mc_pdlp_options* o = &S->o;
+    if (S->trivial) {
+        res->status = MC_PDLP_OPTIMAL;
+        res->tolerance = o->primal_tolerance;
+        fill_message(res, "trivial");
+        res->total_ms = now_ms() - S->t_begin;
+        ctx.drop_session();
+        return MC_OK;
+    }
+    cudaStream_t s = ctx.stream;
+    const int m = S->m, n = S->n;
+    const bool mixed = S->mixed, dev_in = S->dev_in;
+    const long long R = o->restart_every;
+    if (mixed) TRY(finish_chunks(ctx, S->emx, S->loop, o->max_iterations, R, S->ctl, S->tr));
+    else TRY(finish_chunks(ctx, S->e64, S->loop, o->max_iterations, R, S->ctl, S->tr));
+    DevState* st = S->st;
+    mc_pdlp_trace* trace = S->trace;
+    const long long trace_cap = trace ? trace->capacity : 0;
     CU(cudaMemcpy(&ctx.h_state[2], st, sizeof(DevState), cudaMemcpyDeviceToHost));
     CU(cudaEventRecord(ctx.ev_c, s));
 
     // ---- outputs
     const bool dev_out = dev_in;
-    double* xo = dev_out ? x_out : (x_out ? x_stage : nullptr);
-    double* yo = dev_out ? y_out : (y_out ? y_stage : nullptr);
+    double* xo = dev_out ? x_out : (x_out ? S->x_stage : nullptr);
+    double* yo = dev_out ? y_out : (y_out ? S->y_stage : nullptr);
     if (xo || yo) {
         const int nb = blocks_for(ctx, (long long)n + m, kBlock);
         ctx.begin_launch(MC_KERNEL_OTHER);
-        if (mixed) k_unscale_out_mx<<<nb, kBlock, 0, s>>>(n, m, x, fx_avg, y, fy_avg, col_scale, row_scale, xo, yo);
-        else k_unscale_out<<<nb, kBlock, 0, s>>>(n, m, x_avg, y_avg, col_scale, row_scale, xo, yo);
+        if (mixed)
+            k_unscale_out_mx<<<nb, kBlock, 0, s>>>(n, m, S->x, S->fx_avg, S->y, S->fy_avg, S->col_scale,
+                                                   S->row_scale, xo, yo);
+        else k_unscale_out<<<nb, kBlock, 0, s>>>(n, m, S->x_avg, S->y_avg, S->col_scale, S->row_scale, xo, yo);
         ctx.end_launch();
         TRY(ctx.launch_check("unscale"));
     }
     cudaEvent_t ev_d2h = ctx.ev_d;
     CU(cudaEventRecord(ctx.ev_c, s));
     if (!dev_out) {
-        if (x_out) CU(cudaMemcpyAsync(x_out, x_stage, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, s));
-        if (y_out) CU(cudaMemcpyAsync(y_out, y_stage, sizeof(double) * (size_t)m, cudaMemcpyDeviceToHost, s));
+        if (x_out) CU(cudaMemcpyAsync(x_out, S->x_stage, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, s));
+        if (y_out) CU(cudaMemcpyAsync(y_out, S->y_stage, sizeof(double) * (size_t)m, cudaMemcpyDeviceToHost, s));
     }
     CU(cudaMemcpyAsync(&ctx.h_state[3], st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
     CU(cudaEventRecord(ev_d2h, s));
     CU(cudaStreamSynchronize(s));
     TRY(ctx.drain_profile());
-    const DevState& S = ctx.h_state[3];
+    const DevState& DS = ctx.h_state[3];
     if (trace && trace_cap > 0) {
-        const long long cnt = std::min<long long>(S.checks, trace_cap);
+        const long long cnt = std::min<long long>(DS.checks, trace_cap);
         trace->count = cnt;
+        const TraceBuf& tb = S->tr;
         if (cnt > 0) {
-            CU(cudaMemcpy(trace->iteration, at(o_tr_it), sizeof(long long) * cnt, cudaMemcpyDeviceToHost));
-            CU(cudaMemcpy(trace->primal_infeasibility, at(o_tr[0]), sizeof(double) * cnt, cudaMemcpyDeviceToHost));
-            CU(cudaMemcpy(trace->dual_infeasibility, at(o_tr[1]), sizeof(double) * cnt, cudaMemcpyDeviceToHost));
-            CU(cudaMemcpy(trace->duality_gap, at(o_tr[2]), sizeof(double) * cnt, cudaMemcpyDeviceToHost));
-            CU(cudaMemcpy(trace->step_size, at(o_tr[3]), sizeof(double) * cnt, cudaMemcpyDeviceToHost));
-            CU(cudaMemcpy(trace->primal_weight, at(o_tr[4]), sizeof(double) * cnt, cudaMemcpyDeviceToHost));
-            CU(cudaMemcpy(trace->restarted, at(o_tr_rs), sizeof(int) * cnt, cudaMemcpyDeviceToHost));
+            CU(cudaMemcpy(trace->iteration, tb.iteration, sizeof(long long) * cnt, cudaMemcpyDeviceToHost));
+            CU(cudaMemcpy(trace->primal_infeasibility, tb.primal, sizeof(double) * cnt, cudaMemcpyDeviceToHost));
+            CU(cudaMemcpy(trace->dual_infeasibility, tb.dual, sizeof(double) * cnt, cudaMemcpyDeviceToHost));
+            CU(cudaMemcpy(trace->duality_gap, tb.gap, sizeof(double) * cnt, cudaMemcpyDeviceToHost));
+            CU(cudaMemcpy(trace->step_size, tb.eta, sizeof(double) * cnt, cudaMemcpyDeviceToHost));
+            CU(cudaMemcpy(trace->primal_weight, tb.omega, sizeof(double) * cnt, cudaMemcpyDeviceToHost));
+            CU(cudaMemcpy(trace->restarted, tb.restarted, sizeof(int) * cnt, cudaMemcpyDeviceToHost));
         }
     }
     float h2d = 0.f, kern = 0.f, d2h = 0.f;
     CU(cudaEventElapsedTime(&h2d, ctx.ev_a, ctx.ev_b));
     CU(cudaEventElapsedTime(&kern, ctx.ev_b, ctx.ev_c));
     CU(cudaEventElapsedTime(&d2h, ctx.ev_c, ev_d2h));
-    res->status = S.status;
-    res->objective = S.objective;
-    res->primal_infeasibility = S.primal_infeas;
-    res->dual_infeasibility = S.dual_infeas;
-    res->duality_gap = S.gap;
+    res->status = DS.status;
+    res->objective = DS.objective;
+    res->primal_infeasibility = DS.primal_infeas;
+    res->dual_infeasibility = DS.dual_infeas;
+    res->duality_gap = DS.gap;
     res->tolerance = o->primal_tolerance;
-    res->iterations = S.iter;
-    fill_message(res, S.status == MC_PDLP_OPTIMAL ? "PDLP converged"
-                      : S.status == MC_PDLP_NUMERICAL_FAILURE ? "non-finite iterate or residual"
+    res->iterations = DS.iter;
+    fill_message(res, DS.status == MC_PDLP_OPTIMAL ? "PDLP converged"
+                      : DS.status == MC_PDLP_NUMERICAL_FAILURE ? "non-finite iterate or residual"
                                                               : "iteration limit reached");
     res->h2d_ms = dev_in ? 0.0 : h2d;
     res->kernel_ms = kern + (dev_in ? h2d : 0.0);
     res->d2h_ms = dev_out ? 0.0 : d2h;
-    res->ruiz_iterations_executed = o->ruiz_scaling ? S.ruiz_passes : 0;
-    res->restarts = S.restarts;
-    res->final_primal_weight = S.omega;
-    res->final_step_size = S.eta;
-    res->refinement_rounds = mixed ? S.restarts : 0;  // each restart re-centres the FP64 base
-    res->inner_iterations = mixed ? S.iter : 0;
+    res->ruiz_iterations_executed = o->ruiz_scaling ? DS.ruiz_passes : 0;
+    res->restarts = DS.restarts;
+    res->final_primal_weight = DS.omega;
+    res->final_step_size = DS.eta;
+    res->refinement_rounds = mixed ? DS.restarts : 0;  // each restart re-centres the FP64 base
+    res->inner_iterations = mixed ? DS.iter : 0;
     long long total = 0;
     for (int q = 0; q < MC_KERNEL_KINDS; ++q) {
         res->launches_by_kind[q] = ctx.launches[q];
@@ -954,8 +1084,22 @@ int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* 
         total += ctx.launches[q];
     }
     res->kernel_launches = total;
-    res->total_ms = now_ms() - t_begin;
+    res->total_ms = now_ms() - S->t_begin;
+    ctx.drop_session();
     return MC_OK;
+}
+
+int solve_lp(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const double* warm_x,
+             const double* warm_y, double* x_out, double* y_out, mc_pdlp_result* res,
+             mc_pdlp_trace* trace) {
+    if (!res) return set_error(MC_ERR_INVALID_ARGUMENT, "result is NULL");
+    std::memset(res, 0, sizeof *res);
+    std::snprintf(res->backend_actually_used, sizeof res->backend_actually_used, "cuda");
+    int rc = begin_session(ctx, lp, o, warm_x, warm_y, trace);
+    if (rc == MC_OK) rc = iterate_session(ctx, LLONG_MAX, nullptr, nullptr);
+    if (rc == MC_OK) rc = finish_session(ctx, x_out, y_out, res);
+    if (rc != MC_OK) ctx.drop_session();
+    return rc;
 }
 
 }  // namespace mc

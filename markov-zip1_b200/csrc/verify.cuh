@@ -173,6 +173,7 @@ static bool tolerance_ok(double v) { return std::isfinite(v) && v >= 0.0 && v <=
 
 int verify_primal(Ctx& ctx, const mc_lp* lp, const double* primal, double claimed, double feas_abs,
                   double feas_rel, double obj_abs, double obj_rel, mc_verify_report* rep) {
+    ctx.drop_session();  // the verifier reuses the arena
     TRY(validate_lp(lp));
     if (!primal && lp->num_cols > 0) return set_error(MC_ERR_INVALID_ARGUMENT, "primal is NULL");
     // Tolerance::validate (primal_verifier.cpp:38-42)

@@ -29,7 +29,7 @@ from .model import Model, ObjectiveSense, from_triplets
 __all__ = [
     "Backend", "RestartStrategy", "PdlpStatus", "Precision", "PdlpOptions", "PdlpResult",
     "Model", "ObjectiveSense", "Context", "solve_pdlp", "EngineError", "EngineUnavailable",
-    "from_triplets", "device_count", "build", "engine_built",
+    "from_triplets", "device_count", "build", "engine_built", "StepwiseSolve", "DeviceModel",
 ]
 
 
@@ -79,8 +79,6 @@ class PdlpOptions:
     precision: Precision = Precision.fp64
     device: int = 0
     profile_kernels: bool = False
-    refine_max_rounds: int = 12
-    refine_inner_tolerance: float = 1e-4
     check_every_chunks: int = 1
     lanes_per_column: int = 0                      # SpMV tuning, 0 = chosen by line length
     lanes_per_row: int = 0
@@ -206,6 +204,14 @@ class Context:
     def handle(self) -> C.c_void_p:
         return self._h
 
+    @property
+    def stream_handle(self) -> int:
+        """The context's cudaStream_t as an integer (every engine kernel of
+        this context runs on it; torch.cuda.ExternalStream wraps it)."""
+        p = C.c_void_p()
+        _raise(self._lib.mc_pdlp_ctx_stream(self._h, C.byref(p)))
+        return int(p.value or 0)
+
     def solve(self, model: Model, options: Optional[PdlpOptions] = None,
               trace_capacity: int = 0) -> PdlpResult:
         """solve_pdlp on host arrays (copies in and out are part of the call)."""
@@ -232,6 +238,14 @@ class Context:
         if model.num_rows == 0 or model.num_cols == 0:
             x, y = np.zeros(0), np.zeros(0)
         return _result_from(res, x, y, trace)
+
+    def begin(self, model, options: Optional[PdlpOptions] = None,
+              trace_capacity: int = 0) -> "StepwiseSolve":
+        """Start a stepwise solve (mc_pdlp_ctx_begin) of a host Model or a
+        DeviceModel: everything before the first iteration.  Drive it with
+        ``iterate(chunks)`` and end it with ``finish()``; the result equals
+        ``solve`` / ``solve_device`` with the same options."""
+        return StepwiseSolve(self, model, options or PdlpOptions(), trace_capacity)
 
     def solve_batch(self, models: list, options: Optional[PdlpOptions] = None,
                     initial_primal: Optional[list] = None, initial_dual: Optional[list] = None) -> list:
@@ -308,6 +322,68 @@ class Context:
             None if dual_out is None else dual_out.data_ptr(), C.addressof(res), None)
         _raise(rc)
         return _result_from(res, primal_out, dual_out)
+
+
+class StepwiseSolve:
+    """A solve driven a few restart chunks at a time (mc_pdlp_ctx_begin /
+    _iterate / _finish).  Host models are copied in at begin; a DeviceModel
+    must stay alive until finish, and its outputs are device tensors."""
+
+    def __init__(self, ctx: Context, model, options: PdlpOptions, trace_capacity: int = 0):
+        self.ctx = ctx
+        self.model = model
+        self.device = isinstance(model, DeviceModel)
+        self._lp = model.to_struct()
+        self._opts = options.to_struct()
+        self._keep = []
+        warm = []
+        for a, size in ((options.initial_primal, model.num_cols), (options.initial_dual, model.num_rows)):
+            if a is None:
+                warm.append(None)
+            elif self.device:
+                warm.append(a.data_ptr())
+                self._keep.append(a)
+            else:
+                arr = np.ascontiguousarray(a, np.float64)
+                if arr.shape != (size,):
+                    raise ValueError("starting point dimension mismatch")
+                self._keep.append(arr)
+                warm.append(arr.ctypes.data)
+        self._trace, self._trace_arrays = (_make_trace(trace_capacity) if trace_capacity > 0
+                                           else (None, None))
+        _raise(ctx._lib.mc_pdlp_ctx_begin(ctx.handle, C.addressof(self._lp), C.addressof(self._opts),
+                                          warm[0], warm[1],
+                                          C.addressof(self._trace) if self._trace is not None else None))
+        self.iterations = 0
+        self.finished = False
+
+    def iterate(self, chunks: int = 1) -> tuple[int, bool]:
+        """Up to `chunks` further restart chunks; (iterations so far, finished)."""
+        it = C.c_int64(0)
+        fin = C.c_int32(0)
+        _raise(self.ctx._lib.mc_pdlp_ctx_iterate(self.ctx.handle, int(chunks), C.byref(it), C.byref(fin)))
+        self.iterations, self.finished = int(it.value), bool(fin.value)
+        return self.iterations, self.finished
+
+    def finish(self, primal_out=None, dual_out=None) -> PdlpResult:
+        """Outputs and result (mc_pdlp_ctx_finish).  Host models: numpy arrays
+        are returned; device models: pass device tensors (or None)."""
+        res = _abi.McPdlpResult()
+        m = self.model
+        if self.device:
+            x, y = primal_out, dual_out
+            xp = None if x is None else x.data_ptr()
+            yp = None if y is None else y.data_ptr()
+        else:
+            x, y = np.zeros(m.num_cols), np.zeros(m.num_rows)
+            xp, yp = x.ctypes.data, y.ctypes.data
+        _raise(self.ctx._lib.mc_pdlp_ctx_finish(self.ctx.handle, xp, yp, C.addressof(res)))
+        tr = self._trace
+        trace = ({k: a[: tr.count].copy() for k, a in self._trace_arrays.items()}
+                 if tr is not None else None)
+        if not self.device and (m.num_rows == 0 or m.num_cols == 0):
+            x, y = np.zeros(0), np.zeros(0)
+        return _result_from(res, x, y, trace)
 
 
 class DeviceModel:

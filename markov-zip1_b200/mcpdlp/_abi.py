@@ -79,8 +79,6 @@ class McPdlpOptions(C.Structure):
         ("precision", C.c_int32),
         ("device", C.c_int32),
         ("profile_kernels", C.c_int32),
-        ("refine_max_rounds", C.c_int32),
-        ("refine_inner_tolerance", C.c_double),
         ("check_every_chunks", C.c_int32),
         ("lanes_per_column", C.c_int32),
         ("lanes_per_row", C.c_int32),
@@ -177,7 +175,5 @@ def default_options_struct() -> McPdlpOptions:
     o.precision = MC_PRECISION_FP64
     o.device = 0
     o.profile_kernels = 0
-    o.refine_max_rounds = 12
-    o.refine_inner_tolerance = 1e-4
     o.check_every_chunks = 1
     return o

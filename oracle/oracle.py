@@ -13,6 +13,7 @@ module, as the checker; the engine never calls it.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import subprocess
 import sys
 from dataclasses import dataclass
@@ -29,7 +30,9 @@ from mcpdlp.model import Model  # noqa: E402
 
 ORACLE_LIB = HERE / "build" / "liboracle_pdlp.so"
 REF_LIB = HERE / "_ref" / "libref_pdlp.so"
-REFERENCE_SOURCES = Path("/root/reference")
+# The reference checkout: MC_REFERENCE_DIR, else the default that
+# oracle/Makefile uses for REF.
+REFERENCE_SOURCES = Path(os.environ.get("MC_REFERENCE_DIR", "/root/reference"))
 
 _VP = C.c_void_p
 
@@ -41,7 +44,8 @@ def build(reference: bool | None = None) -> None:
         reference = (REFERENCE_SOURCES / "src" / "lp" / "first_order" / "pdlp.cpp").exists()
     if reference:
         targets.append("ref")
-    subprocess.run(["make", "-C", str(HERE), *targets], check=True, capture_output=True)
+    subprocess.run(["make", "-C", str(HERE), f"REF={REFERENCE_SOURCES}", *targets], check=True,
+                   capture_output=True)
 
 
 @dataclass

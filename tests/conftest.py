@@ -31,10 +31,11 @@ def _ensure_built() -> None:
     if not (ROOT / "oracle" / "build" / "liboracle_pdlp.so").exists():
         subprocess.run(["make", "-C", str(ROOT / "oracle"), "oracle"], check=True,
                        capture_output=True)
-    ref_src = Path("/root/reference/src/lp/first_order/pdlp.cpp")
+    from oracle import REFERENCE_SOURCES
+    ref_src = REFERENCE_SOURCES / "src" / "lp" / "first_order" / "pdlp.cpp"
     if ref_src.exists() and not (ROOT / "oracle" / "_ref" / "libref_pdlp.so").exists():
-        subprocess.run(["make", "-C", str(ROOT / "oracle"), "ref"], check=True,
-                       capture_output=True)
+        subprocess.run(["make", "-C", str(ROOT / "oracle"), f"REF={REFERENCE_SOURCES}", "ref"],
+                       check=True, capture_output=True)
 
 
 _ensure_built()

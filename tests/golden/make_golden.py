@@ -23,6 +23,13 @@ Writes, next to this script:
 
     python tests/golden/make_golden.py --only simplex   # refresh that section
     python tests/golden/make_golden.py --only netlib    # the published Netlib optima
+    python tests/golden/make_golden.py --only scale     # larger seeded LPs (minutes)
+
+The ``scale`` section holds the reference solve_pdlp on seeded LPs far above
+the unit-test sizes: the 40M-nonzero LP's generator at m = 200,000,
+n = 500,000, 8 nonzeros per column (4M nonzeros), and the precision-stress
+generator at m = 20,000, n = 60,000, 10 nonzeros per column (600k nonzeros),
+each at 1e-4 and 1e-8 (one process per solve; about five minutes of CPU).
 """
 from __future__ import annotations
 
@@ -42,7 +49,7 @@ from mcpdlp import _abi, generators  # noqa: E402
 from mcpdlp.model import Model, from_triplets  # noqa: E402
 import oracle as orc  # noqa: E402
 
-REF = Path("/root/reference")
+REF = orc.REFERENCE_SOURCES   # MC_REFERENCE_DIR, else /root/reference
 NETLIB = ["afiro", "sc50a", "sc50b", "sc105", "blend", "recipe", "scsd1", "scsd6"]
 SYNTHETIC = [  # (name, seed, m, n, k, family)
     ("config0_s1", 1, 1000, 3000, 6, "standard"),
@@ -52,6 +59,10 @@ SYNTHETIC = [  # (name, seed, m, n, k, family)
     ("precision_s1", 1, 300, 900, 10, "precision"),
 ]
 TOLS = [1e-4, 1e-8]
+SCALE = [  # (name, seed, m, n, k, family)
+    ("standard_4m", 1, 200_000, 500_000, 8, "standard"),
+    ("precision_600k", 1, 20_000, 60_000, 10, "precision"),
+]
 TRANSPORT = [  # (seed, suppliers, customers): within the simplex's dense limits
     (1, 20, 30), (2, 20, 30), (3, 25, 35), (4, 30, 40), (5, 40, 50), (6, 40, 60),
 ]
@@ -138,6 +149,37 @@ def simplex_section(ref) -> dict:
     return out
 
 
+def _scale_job(job) -> dict:
+    """One reference solve of a SCALE model at one tolerance (own process)."""
+    import time
+    name, seed, m_, n_, k_, fam, tol = job
+    ref = orc.ReferencePdlp()
+    m = generators.random_lp(seed, m_, n_, k_, fam)
+    t0 = time.perf_counter()
+    r = ref.solve(m, opts(tol))
+    wall = time.perf_counter() - t0
+    opt = m.info["optimum"]
+    out = dict(status=r.status, iterations=r.iterations, objective=r.objective,
+               primal_infeasibility=r.primal_infeasibility, dual_infeasibility=r.dual_infeasibility,
+               duality_gap=r.duality_gap, restarts=r.restarts, wall_s=wall,
+               objective_rel_err_vs_analytic=abs(r.objective - opt) / abs(opt))
+    print(name, f"{tol:g}", out, flush=True)
+    return dict(name=name, tol=f"{tol:g}", digest=model_digest(m), optimum=opt, result=out)
+
+
+def scale_section() -> dict:
+    import multiprocessing as mp
+    jobs = [(*case, tol) for case in SCALE for tol in TOLS]
+    with mp.get_context("spawn").Pool(len(jobs)) as pool:
+        done = pool.map(_scale_job, jobs)
+    out = {}
+    for name, seed, m_, n_, k_, fam in SCALE:
+        mine = [d for d in done if d["name"] == name]
+        out[name] = dict(seed=seed, m=m_, n=n_, k=k_, family=fam, digest=mine[0]["digest"],
+                         optimum=mine[0]["optimum"], results={d["tol"]: d["result"] for d in mine})
+    return out
+
+
 def main() -> None:
     orc.build(reference=True)
     ref = orc.ReferencePdlp()
@@ -148,6 +190,8 @@ def main() -> None:
             golden["simplex"] = simplex_section(ref)
         elif what == "netlib":
             golden["netlib_optimal"] = netlib_optima()
+        elif what == "scale":
+            golden["scale"] = scale_section()
         (HERE / "golden.json").write_text(json.dumps(golden, indent=1, sort_keys=True))
         return
     golden = {"models": {}, "synthetic": {}, "ruiz": {}}
@@ -178,6 +222,7 @@ def main() -> None:
                                                       e["row_lower"], e["row_upper"]))
     golden["simplex"] = simplex_section(ref)
     golden["netlib_optimal"] = netlib_optima()
+    golden["scale"] = scale_section()
     (HERE / "golden.json").write_text(json.dumps(golden, indent=1, sort_keys=True))
 
 
