@@ -36,6 +36,9 @@ def _ensure_built() -> None:
     if ref_src.exists() and not (ROOT / "oracle" / "_ref" / "libref_pdlp.so").exists():
         subprocess.run(["make", "-C", str(ROOT / "oracle"), f"REF={REFERENCE_SOURCES}", "ref"],
                        check=True, capture_output=True)
+    if ref_src.exists() and not (PKG / "binding" / "_build" / "markov-cero-solve").exists():
+        subprocess.run(["make", "-C", str(PKG / "binding"), f"REF={REFERENCE_SOURCES}", "-j8"],
+                       check=True, capture_output=True)
 
 
 _ensure_built()
