@@ -158,11 +158,39 @@ typedef struct mc_pdlp_result {
     int64_t launches_by_kind[MC_KERNEL_KINDS];
     int64_t kernel_launches;          /* engine kernels launched by this solve */
     int32_t warm_start_used;          /* 1 if the solve started from the given warm start */
-    int32_t reserved_i0;
+    int32_t certificate;              /* batched solves, status INFEASIBLE_OR_UNBOUNDED: the
+                                         mc_certificate kind that proves it (else MC_CERT_NONE) */
     double warm_start_score;          /* guard: max(primal, dual, gap) at the warm start */
     double cold_start_score;          /* guard: the same at the cold start */
-    double reserved_d[2];
+    int64_t certificate_index;        /* MC_CERT_CROSSED_BOUNDS: the column; MC_CERT_ROW_ACTIVITY:
+                                         the row (indices of the LP itself); else -1 */
+    double reserved_d1;
 } mc_pdlp_result;
+
+/* Infeasibility certificates of batched solves (no counterpart in the
+ * reference, whose PDLP never returns INFEASIBLE_OR_UNBOUNDED, pdlp.hpp:43).
+ * Each proves that no x satisfies row_lower <= A x <= row_upper and
+ * var_lower <= x <= var_upper:
+ *   CROSSED_BOUNDS: var_lower[j] > var_upper[j] for j = certificate_index.
+ *   ROW_ACTIVITY:   row i = certificate_index cannot be met with every variable
+ *                   in its box: max over the box of (A x)_i < row_lower[i], or
+ *                   min > row_upper[i] (a dual ray y = -e_i or +e_i).
+ *   DUAL_RAY:       dual_out holds a ray y (unscaled, the reference's sign
+ *                   convention: y_i > 0 only on rows with a finite upper
+ *                   bound, y_i < 0 only with a finite lower bound) with
+ *                   g = A^T y and
+ *                     L = sum_j (g_j > 0 ? g_j var_lower[j] : g_j var_upper[j])
+ *                     U = sum_i (y_i > 0 ? y_i row_upper[i] : y_i row_lower[i])
+ *                   all finite and L > U; for every x in the box
+ *                   L <= g.x = y.(A x) <= U would hold if x were feasible.
+ *                   Found by the restart checks: the dual average of a
+ *                   primal infeasible LP diverges along such a ray. */
+enum {
+    MC_CERT_NONE = 0,
+    MC_CERT_CROSSED_BOUNDS = 1,
+    MC_CERT_ROW_ACTIVITY = 2,
+    MC_CERT_DUAL_RAY = 3
+};
 
 /* Optional per-check history (one entry per restart check). */
 typedef struct mc_pdlp_trace {

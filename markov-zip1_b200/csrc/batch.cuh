@@ -337,6 +337,7 @@ int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o,
     const size_t o_st = L.add<DevState>(count + 1);
     const size_t o_off = L.add<double>(2LL * count);
     const size_t o_flags = L.add<int>(count);
+    const size_t o_cert = L.add<int>(2LL * count);
     bool any_warm = false;
     for (int b = 0; b < count; ++b)
         any_warm = any_warm || (x0 && x0[b] && lps[b].num_cols > 0) || (y0 && y0[b] && lps[b].num_rows > 0);
@@ -398,6 +399,7 @@ int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o,
     double* offsets = static_cast<double*>(at(o_off));
     double* signs = offsets + count;
     int* flags = static_cast<int*>(at(o_flags));
+    int* cert_idx = static_cast<int*>(at(o_cert));
     double* x_work[4];
     for (int q = 0; q < 4; ++q) x_work[q] = static_cast<double*>(at(o_it_n[q]));
     double* y_work[3];
@@ -476,6 +478,7 @@ int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o,
     CU(cudaMemsetAsync(ci + nnz, 0, sizeof(int) * 16, s));
     CU(cudaMemsetAsync(rv + nnz, 0, sizeof(double) * 16, s));
     CU(cudaMemsetAsync(flags, 0, sizeof(int) * count, s));
+    CU(cudaMemsetAsync(cert_idx, 0x7f, sizeof(int) * 2 * (size_t)count, s));  // "none" above any index
     CU(cudaMemsetAsync(st, 0, sizeof(DevState) * (count + 1), s));
     CU(cudaEventRecord(ctx.ev_b, s));
     int bad = 0;
@@ -488,6 +491,7 @@ int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o,
     B.st = st;
     B.offset = offsets;
     B.flags = flags;
+    B.cert_idx = cert_idx;
     B.nlp = count;
     B.warm = warm;
     B.warm_x = warm_x;
@@ -712,6 +716,8 @@ int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o,
     }
     std::vector<DevState> hs(count);
     CU(cudaMemcpyAsync(hs.data(), st, sizeof(DevState) * count, cudaMemcpyDeviceToHost, s));
+    std::vector<int> hcert(2 * (size_t)count);
+    CU(cudaMemcpyAsync(hcert.data(), cert_idx, sizeof(int) * hcert.size(), cudaMemcpyDeviceToHost, s));
     CU(cudaEventRecord(ctx.ev_d, s));
     CU(cudaStreamSynchronize(s));
     TRY(ctx.drain_profile());
@@ -726,6 +732,7 @@ int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o,
         mc_pdlp_result& r = results[b];
         std::snprintf(r.backend_actually_used, sizeof r.backend_actually_used, "cuda");
         r.tolerance = o->primal_tolerance;
+        r.certificate_index = -1;
         if (lps[b].num_rows == 0 || lps[b].num_cols == 0) {
             r.status = MC_PDLP_OPTIMAL;
             fill_message(&r, "trivial");
@@ -738,8 +745,14 @@ int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o,
         r.dual_infeasibility = S.dual_infeas;
         r.duality_gap = S.gap;
         r.iterations = S.iter;
+        r.certificate = S.status == MC_PDLP_INFEASIBLE_OR_UNBOUNDED ? S.cert : MC_CERT_NONE;
+        r.certificate_index = r.certificate == MC_CERT_CROSSED_BOUNDS ? hcert[b]
+                              : r.certificate == MC_CERT_ROW_ACTIVITY ? hcert[count + b]
+                                                                      : -1;
         fill_message(&r, S.status == MC_PDLP_OPTIMAL ? "PDLP converged"
-                         : S.status == MC_PDLP_INFEASIBLE_OR_UNBOUNDED ? "infeasible: certified at setup"
+                         : r.certificate == MC_CERT_CROSSED_BOUNDS ? "infeasible: crossed variable bounds"
+                         : r.certificate == MC_CERT_ROW_ACTIVITY ? "infeasible: row activity outside its bounds"
+                         : r.certificate == MC_CERT_DUAL_RAY ? "infeasible: dual ray (Farkas certificate in dual)"
                          : S.status == MC_PDLP_NUMERICAL_FAILURE ? "non-finite iterate or residual"
                                                                  : "iteration limit reached");
         r.h2d_ms = h2d;

@@ -44,6 +44,8 @@ struct BatchRefs {
     DevState* st;              // [nlp]
     const double* offset;      // [nlp] objective offsets
     int* flags;                // [nlp] setup certificates: 1 crossed bounds, 2 row activity
+    int* cert_idx;             // [2 nlp] lowest crossed column, lowest failing row of each LP
+                               // (LP-local indices; INT_MAX if none)
     const int* warm;           // [nlp] starting point given: 1 primal, 2 dual (NULL: none)
     const double* warm_x;      // [n] packed starting primal (original space)
     const double* warm_y;      // [m] packed starting dual
@@ -67,6 +69,60 @@ struct BatchRefs {
     for (int base_ = TT.l0[T], LINE = 0;                                                            \
          base_ < tl1_ && ((LINE = base_ + (int)(threadIdx.x / G)), true); base_ += kBlock / G)     \
         if (const bool VALID = LINE < tl1_; true)
+
+// The Farkas test of the dual average, evaluated in the residual pass on the
+// unscaled y = y_avg and g = A^T y (the residual pass's own product, without
+// c).  For any x in the variable box that met the rows,
+//     L = sum_j (g_j > 0 ? g_j lo_j : g_j hi_j) <= g.x = y.(A x) <= U,
+//     U = sum_i (y_i > 0 ? y_i hi_i : y_i lo_i) = -(the row part of the dual
+//         objective, RowTerms::dsum),
+// so L > U proves the LP infeasible.  The dual update's projection keeps the
+// signs of y consistent with the finite row bounds; a nonzero term meeting an
+// infinite bound makes the side infinite and is counted instead.  The scales
+// bound the rounding of both sums (|bound| times sum |a y| per column, |y
+// bound| per row), so a margin of 1e-9 of them cannot come from rounding.
+struct RayTerms {
+    double l = 0.0, cscale = 0.0, cinf = 0.0, rscale = 0.0, rinf = 0.0;
+    __device__ __forceinline__ void add_col(const Original& O, int j, double s, double s_abs) {
+        const double g = __ddiv_rn(s, O.col_scale[j]);
+        const double gabs = s_abs / O.col_scale[j];
+        const double lo = O.lo[j], hi = O.hi[j];
+        if (g != 0.0) {
+            const double bnd = (g > 0.0) ? lo : hi;
+            if (fabs(bnd) >= 1e299) {
+                cinf += 1.0;
+            } else {
+                l += __dmul_rn(g, bnd);
+                cscale += gabs * fabs(bnd);
+            }
+        }
+    }
+    __device__ __forceinline__ void add_row(const Original& O, int i, double y_scaled) {
+        const double yu = __dmul_rn(y_scaled, O.row_scale[i]);
+        if (yu == 0.0) return;
+        const double bnd = (yu > 0.0) ? O.bhi[i] : O.blo[i];
+        if (fabs(bnd) >= 1e299) rinf += 1.0;
+        else rscale += fabs(yu * bnd);
+    }
+    __device__ __forceinline__ void store_cols(double* partials, double* scratch, int t) {
+        l = block_reduce(l, scratch, OpSum());
+        cscale = block_reduce(cscale, scratch, OpSum());
+        cinf = block_reduce(cinf, scratch, OpSum());
+        if (threadIdx.x == 0) {
+            partials[SLOT_RAY_L * kMaxTiles + t] = l;
+            partials[SLOT_RAY_CSCALE * kMaxTiles + t] = cscale;
+            partials[SLOT_RAY_CINF * kMaxTiles + t] = cinf;
+        }
+    }
+    __device__ __forceinline__ void store_rows(double* partials, double* scratch, int t) {
+        rscale = block_reduce(rscale, scratch, OpSum());
+        rinf = block_reduce(rinf, scratch, OpSum());
+        if (threadIdx.x == 0) {
+            partials[SLOT_RAY_RSCALE * kMaxTiles + t] = rscale;
+            partials[SLOT_RAY_RINF * kMaxTiles + t] = rinf;
+        }
+    }
+};
 
 // ------------------------------------------------------------------ primal
 template <int G, bool STEP, class T>
@@ -188,6 +244,7 @@ __global__ void __launch_bounds__(kBlock) kb_residual_rows(Iterates<double> P, O
     __shared__ double scratch[32];
     MC_FOR_ACTIVE(B, 1, t) {
         RowTerms acc;
+        RayTerms ray;
         MC_TILE_LINES(B.rows, t, i, valid, sub) {
             double s = 0.0;
             if (valid) {
@@ -195,7 +252,10 @@ __global__ void __launch_bounds__(kBlock) kb_residual_rows(Iterates<double> P, O
                 for (int p = b + sub; p < e; p += G) s = fma(P.csr_val[p], P.x_avg[P.csr_col[p]], s);
             }
             s = group_sum<G>(s);
-            if (valid && sub == 0) acc.add(O, i, s, P.y_avg[i]);
+            if (valid && sub == 0) {
+                acc.add(O, i, s, P.y_avg[i]);
+                ray.add_row(O, i, P.y_avg[i]);
+            }
         }
         acc.vmax = block_reduce(acc.vmax, scratch, OpMax());
         acc.dsum = block_reduce(acc.dsum, scratch, OpSum());
@@ -205,6 +265,7 @@ __global__ void __launch_bounds__(kBlock) kb_residual_rows(Iterates<double> P, O
             P.partials[SLOT_ROW_DOBJ * kMaxTiles + t] = acc.dsum;
             P.partials[SLOT_NAN * kMaxTiles + t] = acc.bad;
         }
+        ray.store_rows(P.partials, scratch, t);
     }
 }
 
@@ -213,14 +274,23 @@ __global__ void __launch_bounds__(kBlock) kb_residual_cols(Iterates<double> P, O
     __shared__ double scratch[32];
     MC_FOR_ACTIVE(B, 0, t) {
         ColTerms acc;
+        RayTerms ray;
         MC_TILE_LINES(B.cols, t, j, valid, sub) {
-            double s = 0.0;
+            double s = 0.0, sa = 0.0;
             if (valid) {
                 const int b = P.csc_start[j], e = P.csc_start[j + 1];
-                for (int p = b + sub; p < e; p += G) s = fma(P.csc_val[p], P.y_avg[P.csc_row[p]], s);
+                for (int p = b + sub; p < e; p += G) {
+                    const double a = P.csc_val[p], yv = P.y_avg[P.csc_row[p]];
+                    s = fma(a, yv, s);
+                    sa = fma(fabs(a), fabs(yv), sa);
+                }
             }
             s = group_sum<G>(s);
-            if (valid && sub == 0) acc.add(O, j, s, P.x_avg[j]);
+            sa = group_sum<G>(sa);
+            if (valid && sub == 0) {
+                acc.add(O, j, s, P.x_avg[j]);
+                ray.add_col(O, j, s, sa);
+            }
         }
         acc.vmax = block_reduce(acc.vmax, scratch, OpMax());
         acc.dres = block_reduce(acc.dres, scratch, OpSum());
@@ -234,6 +304,7 @@ __global__ void __launch_bounds__(kBlock) kb_residual_cols(Iterates<double> P, O
             P.partials[SLOT_COL_DOBJ * kMaxTiles + t] = acc.dobj;
             P.partials[SLOT_B * kMaxTiles + t] = acc.bad;
         }
+        ray.store_cols(P.partials, scratch, t);
     }
 }
 
@@ -255,8 +326,16 @@ __global__ void kb_finalize(const double* __restrict__ partials, BatchRefs B, lo
     const double col_pobj = reduce_partials(partials + SLOT_COL_POBJ * kMaxTiles + c0, nc, scratch, OpSum());
     const double col_dobj = reduce_partials(partials + SLOT_COL_DOBJ * kMaxTiles + c0, nc, scratch, OpSum());
     const double bad_c = reduce_partials(partials + SLOT_B * kMaxTiles + c0, nc, scratch, OpSum());
+    const double ray_l = reduce_partials(partials + SLOT_RAY_L * kMaxTiles + c0, nc, scratch, OpSum());
+    const double ray_cs = reduce_partials(partials + SLOT_RAY_CSCALE * kMaxTiles + c0, nc, scratch, OpSum());
+    const double ray_ci = reduce_partials(partials + SLOT_RAY_CINF * kMaxTiles + c0, nc, scratch, OpSum());
+    const double ray_rs = reduce_partials(partials + SLOT_RAY_RSCALE * kMaxTiles + r0, nr, scratch, OpSum());
+    const double ray_ri = reduce_partials(partials + SLOT_RAY_RINF * kMaxTiles + r0, nr, scratch, OpSum());
     if (threadIdx.x != 0) return;
     const double offset = B.offset[lp];
+    // the Farkas test of the dual average (RayTerms): U = -row_dobj
+    const double margin = ray_l + row_dobj;
+    const bool farkas = ray_ci == 0.0 && ray_ri == 0.0 && margin > 0.0 && margin > 1e-9 * (ray_cs + ray_rs);
     const double primal = maxv(row_max, col_max);
     const double dual = sqrt(col_dres) / st->c_scale;
     const double pobj = offset + col_pobj;
@@ -278,6 +357,10 @@ __global__ void kb_finalize(const double* __restrict__ partials, BatchRefs B, lo
     } else if (!final_pass && primal <= ctl.primal_tol && dual <= ctl.dual_tol && gap <= ctl.gap_tol) {
         st->done = 1;
         st->status = 0;
+    } else if (farkas) {
+        st->done = 1;
+        st->status = 2;           // infeasible_or_unbounded, the dual average is the ray
+        st->cert = MC_CERT_DUAL_RAY;
     } else if (!final_pass) {
         const bool do_restart =
             ctl.strategy == 2 ||
@@ -400,7 +483,10 @@ __global__ void kb_setup_cols(const int* __restrict__ col_start, const double* _
         const_cast<double*>(P.hi)[j] = hsent;
         const_cast<double*>(O.lo)[j] = isinf(l0) ? -kBig : l0;
         const_cast<double*>(O.hi)[j] = isinf(h0) ? kBig : h0;
-        if (l0 > h0) crossed = 1;
+        if (l0 > h0 && !crossed) {
+            crossed = 1;
+            atomicMin(B.cert_idx + lp, j - B.cols.l0[B.cols.first[lp]]);
+        }
         const double cj = sign * __dmul_rn(obj_in[j], s);
         const_cast<double*>(P.c)[j] = cj;
         cmax = maxv(cmax, fabs(cj));
@@ -465,7 +551,10 @@ __global__ void kb_setup_rows(const int* __restrict__ row_start, const int* __re
         }
         const_cast<double*>(P.row_norm)[i] = (nrm < 1e-12) ? 1.0 : nrm;
         const double slack = 1e-9 * (1.0 + mag + maxv(isfinite(l0) ? fabs(l0) : 0.0, isfinite(h0) ? fabs(h0) : 0.0));
-        if ((isfinite(l0) && amax < l0 - slack) || (isfinite(h0) && amin > h0 + slack)) infeasible = 1;
+        if ((isfinite(l0) && amax < l0 - slack) || (isfinite(h0) && amin > h0 + slack)) {
+            if (!infeasible) atomicMin(B.cert_idx + B.nlp + lp, i - B.rows.l0[B.rows.first[lp]]);
+            infeasible = 1;
+        }
         const double y0 = (B.warm && (B.warm[lp] & 2)) ? __dmul_rn(B.warm_y[i], 1.0 / s) : 0.0;
         P.y[i] = y0;
         P.y_avg[i] = y0;
@@ -508,9 +597,11 @@ __global__ void kb_setup_scalars(const double* __restrict__ partials, BatchRefs 
         if (B.flags[lp]) {
             st->done = 1;
             st->status = 2;  // infeasible_or_unbounded, certified at setup
+            st->cert = (B.flags[lp] & 1) ? MC_CERT_CROSSED_BOUNDS : MC_CERT_ROW_ACTIVITY;
         } else {
             st->done = 0;
             st->status = 1;
+            st->cert = MC_CERT_NONE;
         }
     }
 }
@@ -667,6 +758,7 @@ __global__ void __launch_bounds__(kBlock) kb_residual_rows_mx(Iterates<float> P,
     __shared__ double scratch[32];
     MC_FOR_ACTIVE(B, 1, t) {
         RowTerms acc;
+        RayTerms ray;
         MC_TILE_LINES(B.rows, t, i, valid, sub) {
             double s = 0.0;
             if (valid) {
@@ -679,7 +771,9 @@ __global__ void __launch_bounds__(kBlock) kb_residual_rows_mx(Iterates<float> P,
             s = group_sum<G>(s);
             if (valid && sub == 0) {
                 M.ax_full[i] = s;
-                acc.add(O, i, s, M.y_hat[i] + (double)P.y_avg[i]);
+                const double yv = M.y_hat[i] + (double)P.y_avg[i];
+                acc.add(O, i, s, yv);
+                ray.add_row(O, i, yv);
             }
         }
         acc.vmax = block_reduce(acc.vmax, scratch, OpMax());
@@ -690,6 +784,7 @@ __global__ void __launch_bounds__(kBlock) kb_residual_rows_mx(Iterates<float> P,
             P.partials[SLOT_ROW_DOBJ * kMaxTiles + t] = acc.dsum;
             P.partials[SLOT_NAN * kMaxTiles + t] = acc.bad;
         }
+        ray.store_rows(P.partials, scratch, t);
     }
 }
 
@@ -699,19 +794,24 @@ __global__ void __launch_bounds__(kBlock) kb_residual_cols_mx(Iterates<float> P,
     __shared__ double scratch[32];
     MC_FOR_ACTIVE(B, 0, t) {
         ColTerms acc;
+        RayTerms ray;
         MC_TILE_LINES(B.cols, t, j, valid, sub) {
-            double s = 0.0;
+            double s = 0.0, sa = 0.0;
             if (valid) {
                 const int b = P.csc_start[j], e = P.csc_start[j + 1];
                 for (int p = b + sub; p < e; p += G) {
                     const int ii = P.csc_row[p];
-                    s = fma(M.csc_val64[p], M.y_hat[ii] + (double)P.y_avg[ii], s);
+                    const double a = M.csc_val64[p], yv = M.y_hat[ii] + (double)P.y_avg[ii];
+                    s = fma(a, yv, s);
+                    sa = fma(fabs(a), fabs(yv), sa);
                 }
             }
             s = group_sum<G>(s);
+            sa = group_sum<G>(sa);
             if (valid && sub == 0) {
                 M.aty_full[j] = s;
                 acc.add(O, j, s, M.x_hat[j] + (double)P.x_avg[j]);
+                ray.add_col(O, j, s, sa);
             }
         }
         acc.vmax = block_reduce(acc.vmax, scratch, OpMax());
@@ -726,6 +826,7 @@ __global__ void __launch_bounds__(kBlock) kb_residual_cols_mx(Iterates<float> P,
             P.partials[SLOT_COL_DOBJ * kMaxTiles + t] = acc.dobj;
             P.partials[SLOT_B * kMaxTiles + t] = acc.bad;
         }
+        ray.store_cols(P.partials, scratch, t);
     }
 }
 

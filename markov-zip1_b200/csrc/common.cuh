@@ -31,7 +31,13 @@ enum PartialSlot : int {
     SLOT_B = 9,
     SLOT_C = 10,
     SLOT_NAN = 11,      // count of non-finite values seen in a residual pass
-    NUM_SLOTS = 12
+    // batch residual pass: the Farkas test of the dual average (batch_kernels.cuh)
+    SLOT_RAY_L = 12,       // sum_j (g_j > 0 ? g_j lo_j : g_j hi_j), g = A^T y_avg     (columns)
+    SLOT_RAY_CSCALE = 13,  // sum_j |bound_j| sum_i |a_ij y_i|: rounding scale        (columns)
+    SLOT_RAY_CINF = 14,    // count of nonzero g_j meeting an infinite bound           (columns)
+    SLOT_RAY_RSCALE = 15,  // sum_i |y_i bound_i|                                      (rows)
+    SLOT_RAY_RINF = 16,    // count of nonzero y_i meeting an infinite bound           (rows)
+    NUM_SLOTS = 17
 };
 
 // Scalars of one solve, resident in device memory so that whole restart
@@ -54,7 +60,8 @@ struct DevState {
     int ruiz_done;                  // Ruiz converged: later passes are no-ops
     int nonfinite;                  // a residual pass saw NaN/Inf
     int active_tiles[2];            // batch poll state: running column / row tiles
-    int pad;
+    int cert;                       // batch: MC_CERT_* kind when status is infeasible
+    int pad[3];
 };
 
 // ---- cache policy helpers -------------------------------------------------

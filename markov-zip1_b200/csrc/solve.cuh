@@ -994,6 +994,8 @@ int finish_session(Ctx& ctx, double* x_out, double* y_out, mc_pdlp_result* res) 
     if (!res) return set_error(MC_ERR_INVALID_ARGUMENT, "result is NULL");
     std::memcpy(res, &S->head, sizeof *res);
     std::snprintf(res->backend_actually_used, sizeof res->backend_actually_used, "cuda");
+    res->certificate = MC_CERT_NONE;  // a single solve keeps the reference's statuses (no certificates)
+    res->certificate_index = -1;
     const mc_pdlp_options* o = &S->o;
     if (S->trivial) {
         res->status = MC_PDLP_OPTIMAL;

@@ -139,6 +139,8 @@ def _result_from(r: _abi.McPdlpResult, x, y, trace=None) -> PdlpResult:
         warm_start_used=bool(r.warm_start_used),
         warm_start_score=r.warm_start_score,
         cold_start_score=r.cold_start_score,
+        certificate=_abi.CERTIFICATE_NAMES[r.certificate] if 0 <= r.certificate < 4 else str(r.certificate),
+        certificate_index=r.certificate_index,
         launches_by_kind={n: r.launches_by_kind[i] for i, n in enumerate(_abi.KERNEL_KIND_NAMES)
                           if n != "-"},
         kernel_ms_by_kind={n: r.kernel_ms_by_kind[i] for i, n in enumerate(_abi.KERNEL_KIND_NAMES)

@@ -32,6 +32,7 @@ MC_MEMORY_DEVICE = 1
 MC_PRECISION_FP64 = 0
 MC_PRECISION_FP32_REFINE = 1
 MC_KERNEL_KINDS = 8
+CERTIFICATE_NAMES = ("none", "crossed_bounds", "row_activity", "dual_ray")
 KERNEL_KIND_NAMES = ("primal", "dual", "dual_step", "residual", "setup", "other", "-", "-")
 
 _P_i32 = C.POINTER(C.c_int32)
@@ -113,10 +114,11 @@ class McPdlpResult(C.Structure):
         ("launches_by_kind", C.c_int64 * MC_KERNEL_KINDS),
         ("kernel_launches", C.c_int64),
         ("warm_start_used", C.c_int32),
-        ("reserved_i0", C.c_int32),
+        ("certificate", C.c_int32),
         ("warm_start_score", C.c_double),
         ("cold_start_score", C.c_double),
-        ("reserved_d", C.c_double * 2),
+        ("certificate_index", C.c_int64),
+        ("reserved_d1", C.c_double),
     ]
 
 
