@@ -317,6 +317,30 @@ int mc_pdlp_ctx_solve_batch_warm(mc_pdlp_ctx* ctx, const mc_lp* lps, int32_t cou
                                  double* const* dual_out, mc_pdlp_result* results);
 
 /*
+ * Variants of one LP that differ only in their variable bounds -- the nodes
+ * of one branching round of branch and bound, which tighten bounds of the
+ * parent LP (src/milp/milp_solver.cpp:401-447) -- solved together with the
+ * matrix read once per iteration for all of them (no counterpart in the
+ * reference, which solves one node LP per call, src/milp/node_lp.cpp:9-82).
+ * `base` gives A, the objective, the row bounds and default variable bounds;
+ * variant b replaces the variable bounds by var_lower[b] / var_upper[b]
+ * (num_cols each, host or device memory; a NULL array or entry keeps the
+ * base's).  initial_primal / initial_dual (may be NULL, or hold NULL
+ * entries) give starting points in original units, as for
+ * mc_pdlp_ctx_solve_batch_warm.  Every variant runs the algorithm of
+ * mc_pdlp_ctx_solve on its own LP (own step size, primal weight, restarts,
+ * termination); results[b], primal_out[b] / dual_out[b] (may be NULL) as for
+ * the batch.  Infeasible variants end with INFEASIBLE_OR_UNBOUNDED and a
+ * certificate (crossed bounds, row activity, or a dual ray in dual_out[b]).
+ * FP64 form only.
+ */
+int mc_pdlp_ctx_solve_variants(mc_pdlp_ctx* ctx, const mc_lp* base, int32_t count,
+                               const double* const* var_lower, const double* const* var_upper,
+                               const mc_pdlp_options* options, const double* const* initial_primal,
+                               const double* const* initial_dual, double* const* primal_out,
+                               double* const* dual_out, mc_pdlp_result* results);
+
+/*
  * Learned warm start (no counterpart in the reference): a bipartite
  * message-passing network over an LP's constraint/variable graph (hidden 64,
  * `rounds` rounds, FP32) that predicts a primal/dual starting point and the

@@ -84,9 +84,12 @@ struct BatchRefs {
 struct RayTerms {
     double l = 0.0, cscale = 0.0, cinf = 0.0, rscale = 0.0, rinf = 0.0;
     __device__ __forceinline__ void add_col(const Original& O, int j, double s, double s_abs) {
+        add_col_b(O, j, s, s_abs, O.lo[j], O.hi[j]);
+    }
+    __device__ __forceinline__ void add_col_b(const Original& O, int j, double s, double s_abs, double lo,
+                                              double hi) {
         const double g = __ddiv_rn(s, O.col_scale[j]);
         const double gabs = s_abs / O.col_scale[j];
-        const double lo = O.lo[j], hi = O.hi[j];
         if (g != 0.0) {
             const double bnd = (g > 0.0) ? lo : hi;
             if (fabs(bnd) >= 1e299) {

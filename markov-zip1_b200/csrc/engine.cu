@@ -184,6 +184,7 @@ int pick_lanes(double mean_len) {
 
 #include "solve.cuh"
 #include "batch.cuh"
+#include "variants.cuh"
 #include "kernel_api.cuh"
 #include "verify.cuh"
 
@@ -334,6 +335,17 @@ int mc_pdlp_ctx_solve_batch_warm(mc_pdlp_ctx* c, const mc_lp* lps, int32_t count
     if (!ctx) return set_error(MC_ERR_INVALID_ARGUMENT, "context is NULL");
     DeviceGuard guard(ctx->device);
     return solve_batch(*ctx, lps, count, options, initial_primal, initial_dual, primal_out, dual_out, results);
+}
+
+int mc_pdlp_ctx_solve_variants(mc_pdlp_ctx* c, const mc_lp* base, int32_t count, const double* const* var_lower,
+                               const double* const* var_upper, const mc_pdlp_options* options,
+                               const double* const* initial_primal, const double* const* initial_dual,
+                               double* const* primal_out, double* const* dual_out, mc_pdlp_result* results) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(c);
+    if (!ctx) return set_error(MC_ERR_INVALID_ARGUMENT, "context is NULL");
+    DeviceGuard guard(ctx->device);
+    return solve_variants(*ctx, base, count, var_lower, var_upper, options, initial_primal, initial_dual,
+                          primal_out, dual_out, results);
 }
 
 int mc_pdlp_solve(const mc_lp* lp, const mc_pdlp_options* options, const double* initial_primal,

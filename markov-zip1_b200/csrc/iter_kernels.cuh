@@ -391,9 +391,13 @@ struct RowTerms {
 struct ColTerms {
     double vmax = 0.0, dres = 0.0, pobj = 0.0, dobj = 0.0, bad = 0.0;
     __device__ __forceinline__ void add(const Original& O, int j, double s, double x_scaled) {
+        add_b(O, j, s, x_scaled, O.lo[j], O.hi[j]);
+    }
+    // the same with the column's (original, sentinel-form) bounds given
+    __device__ __forceinline__ void add_b(const Original& O, int j, double s, double x_scaled, double lo,
+                                          double hi) {
         const double aty = __ddiv_rn(s, O.col_scale[j]);
         const double xu = __dmul_rn(x_scaled, O.col_scale[j]);
-        const double lo = O.lo[j], hi = O.hi[j];
         const double proj = clampv(xu, lo, hi);
         const double r = fabs(xu - proj);
         const double sc = 1.0 + maxv(fabs(xu), fabs(proj) < 1e299 ? fabs(proj) : 0.0);

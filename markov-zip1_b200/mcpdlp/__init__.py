@@ -290,6 +290,45 @@ class Context:
                                                           C.addressof(yp), C.addressof(res)))
         return [_result_from(res[b], xs[b], ys[b]) for b in range(count)]
 
+    def solve_variants(self, base: Model, var_lower: list, var_upper: list,
+                       options: Optional[PdlpOptions] = None, initial_primal: Optional[list] = None,
+                       initial_dual: Optional[list] = None) -> list:
+        """Solve variants of `base` that differ only in their variable bounds
+        (mc_pdlp_ctx_solve_variants): var_lower[b] / var_upper[b] are arrays
+        of num_cols (None keeps the base's).  One PdlpResult per variant."""
+        options = options or PdlpOptions()
+        o = options.to_struct()
+        count = len(var_lower)
+        if len(var_upper) != count or count == 0:
+            raise ValueError("var_lower and var_upper need one entry per variant")
+        n, m = base.num_cols, base.num_rows
+        keep = []
+
+        def ptrs(given, size):
+            out = (C.c_void_p * count)()
+            for b in range(count):
+                v = None if given is None else given[b]
+                if v is not None:
+                    a = np.ascontiguousarray(v, dtype=np.float64)
+                    if a.shape != (size,):
+                        raise ValueError("variant array dimension mismatch")
+                    keep.append(a)
+                    out[b] = a.ctypes.data
+            return out
+        lo, hi = ptrs(var_lower, n), ptrs(var_upper, n)
+        x0, y0 = ptrs(initial_primal, n), ptrs(initial_dual, m)
+        xs = [np.zeros(n) for _ in range(count)]
+        ys = [np.zeros(m) for _ in range(count)]
+        xp = (C.c_void_p * count)(*[a.ctypes.data if len(a) else None for a in xs])
+        yp = (C.c_void_p * count)(*[a.ctypes.data if len(a) else None for a in ys])
+        res = (_abi.McPdlpResult * count)()
+        lp = base.to_struct()
+        _raise(self._lib.mc_pdlp_ctx_solve_variants(self._h, C.addressof(lp), count, C.addressof(lo),
+                                                    C.addressof(hi), C.addressof(o), C.addressof(x0),
+                                                    C.addressof(y0), C.addressof(xp), C.addressof(yp),
+                                                    C.addressof(res)))
+        return [_result_from(res[b], xs[b], ys[b]) for b in range(count)]
+
     def verify_primal(self, model: Model, primal, claimed_objective: float,
                       feasibility_tolerance: float = 1e-7, objective_tolerance: float = 1e-7) -> dict:
         """verify_primal (src/verify/primal_verifier.cpp:44) on the device

@@ -57,6 +57,7 @@ ENGINE_SIGNATURES = {
     "mc_pdlp_ctx_iterate": ([_VP, _I64, _VP, _VP], C.c_int),
     "mc_pdlp_ctx_finish": ([_VP, _VP, _VP, _VP], C.c_int),
     "mc_pdlp_ctx_solve_batch": ([_VP, _VP, C.c_int32, _VP, _VP, _VP, _VP], C.c_int),
+    "mc_pdlp_ctx_solve_variants": ([_VP, _VP, C.c_int32, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP], C.c_int),
     "mc_pdlp_ctx_solve_batch_warm": ([_VP, _VP, C.c_int32, _VP, _VP, _VP, _VP, _VP, _VP], C.c_int),
     "mc_gnn_create": ([C.c_int, C.c_int, C.c_uint64, _VP], C.c_int),
     "mc_gnn_destroy": ([_VP], C.c_int),
