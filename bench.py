@@ -311,17 +311,18 @@ def batch_models(workload: str, world: int = 1, rank: int = 0):
         shapes = generators.batch_part1_shapes(1, 256 * world)
         mine = shard_by_nnz([n * k for (_, n, k) in shapes], world)[rank]
         return (generators.batch_part1(1, 256 * world, only=mine),
-                "256 uneven LPs per GPU (m~U[100,20000], n~U[2m,4m], k~U{4..12}), batched, tolerance 1e-6")
+                "256 uneven LPs per GPU (m~U[100,20000], n~U[2m,4m], k~U{4..12}), batched, tolerance 1e-6", None)
     mine = shard_by_nnz([1] * (512 * world), world)[rank]
-    _, models, _ = generators.batch_part2(1, 512 * world, only=mine)
-    return models, "512 node variants per GPU of one LP (m=5000, n=15000, 8 nnz/col), batched, tolerance 1e-6"
+    base, models, _ = generators.batch_part2(1, 512 * world, only=mine)
+    return (models, "512 node variants per GPU of one LP (m=5000, n=15000, 8 nnz/col), batched, tolerance 1e-6",
+            base)
 
 
 def run_batch_ncu_case(args) -> None:
     """A short batched solve of the batch workload (for ncu captures)."""
     import mcpdlp
     from mcpdlp import PdlpOptions, Precision
-    models, _ = batch_models(args.workload)
+    models, _, _ = batch_models(args.workload)
     ctx = mcpdlp.Context(0)
     o = PdlpOptions(max_iterations=args.ncu_iterations, profile_kernels=True,
                     precision=Precision.fp32_refine if args.precision == "fp32_refine" else Precision.fp64)
@@ -344,34 +345,45 @@ def run_batch_arm(args) -> None:
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     dist = init_dist(world, "nccl")
-    models, label = batch_models(args.workload, world, rank)
+    models, label, base = batch_models(args.workload, world, rank)
     ctx = mcpdlp.Context(local)
     from mcpdlp import Precision
 
-    def timed(precision):
+    def timed(precision, solve=None):
         o = PdlpOptions(device=local, precision=precision)
         o.set_tolerance(1e-6)
+        solve = solve or (lambda: ctx.solve_batch(models, o))
         for _ in range(args.warmup):
-            ctx.solve_batch(models, o)
+            solve()
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         res = None
         for _ in range(args.steps):
-            res = ctx.solve_batch(models, o)
+            res = solve()
         return max_over_ranks(dist, time.perf_counter() - t0, dev), res
 
     # the FP32 + FP64-refinement form is the workload's; plain FP64 beside it
     el, res = timed(Precision.fp32_refine)
     el64, res64 = timed(Precision.fp64)
     lps = sum_over_ranks(dist, float(len(models) * args.steps), dev)
+    shared = None
+    if base is not None:
+        # the node variants with the matrix read once per iteration for all of them
+        ov = PdlpOptions(device=local)
+        ov.set_tolerance(1e-6)
+        lows, ups = [m_.var_lower for m_ in models], [m_.var_upper for m_ in models]
+        elv, resv = timed(Precision.fp64, lambda: ctx.solve_variants(base, lows, ups, ov))
+        shared = (elv, resv)
 
     def summary(rs):
         st = [r.status.name for r in rs]
         errs = [abs(r.objective - m.info["optimum"]) / abs(m.info["optimum"]) for r, m in zip(rs, models)
                 if r.status.name == "optimal" and "optimum" in m.info and args.workload == "batch1"]
+        certs = [r.extra["certificate"] for r in rs if r.status.name == "infeasible_or_unbounded"]
         return {"statuses": {k: st.count(k) for k in sorted(set(st))},
+                "certificates": {k: certs.count(k) for k in sorted(set(certs))},
                 "max_iterations_in_batch": max(r.iterations for r in rs),
                 "max_objective_rel_err_vs_analytic": max(errs) if errs else None}
 
@@ -386,6 +398,13 @@ def run_batch_arm(args) -> None:
                       "fp64": {"LPs_per_s": lps / el64, "ms_per_step": el64 * 1e3 / args.steps,
                                **summary(res64)}},
             "gpu_launches": res[0].extra["kernel_launches"] * args.steps}
+    if shared is not None:
+        elv, resv = shared
+        agree = sum(1 for a, b in zip(resv, res64) if a.status == b.status)
+        line["forms"]["shared_matrix_fp64"] = {
+            "LPs_per_s": lps / elv, "ms_per_step": elv * 1e3 / args.steps,
+            "speedup_vs_packed_fp64": el64 / elv, "status_agrees_with_packed": f"{agree}/{len(models)}",
+            "engine": "mc_pdlp_ctx_solve_variants: one matrix, variant-minor iterates", **summary(resv)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()
