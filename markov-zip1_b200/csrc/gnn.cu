@@ -78,18 +78,62 @@ struct Layout {
 
 // ----------------------------------------------------------------- kernels
 // Y[N x H] = act(X1[N x K1] W1[K1 x H] + X2[N x K2] W2[K2 x H] + b)
-__global__ void g_dense_fwd(int N, const float* __restrict__ X1, int K1, const float* __restrict__ W1,
-                            const float* __restrict__ X2, int K2, const float* __restrict__ W2,
-                            const float* __restrict__ b, float* __restrict__ Y, int relu) {
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)N * H;
-         t += (long long)gridDim.x * blockDim.x) {
-        const long long r = t / H;
-        const int c = (int)(t % H);
-        float acc = b[c];
-        for (int k = 0; k < K1; ++k) acc = fmaf(X1[r * K1 + k], W1[k * H + c], acc);
-        if (X2)
-            for (int k = 0; k < K2; ++k) acc = fmaf(X2[r * K2 + k], W2[k * H + c], acc);
-        Y[t] = relu ? fmaxf(acc, 0.f) : acc;
+//
+// Tiled: a block computes a 64-row tile of Y; the weights (K x 64) and the
+// tile's input rows are staged in shared memory once, and each of the 256
+// threads accumulates a 4 x 4 register block (rows ty*4.., columns tx*4..),
+// so every weight and input value is read from global memory once per tile
+// instead of once per output.  Each output sums b, then X1 W1 over k in
+// order, then X2 W2 -- the order of the one-thread-per-output form.
+constexpr int kTile = 64;
+__device__ __forceinline__ void dense_stage(float (*sA)[kTile + 1], float (*sW)[H], const float* __restrict__ A,
+                                            int K, const float* __restrict__ W, long long r0, int rows) {
+    for (int q = threadIdx.x; q < kTile * kTile; q += blockDim.x) {
+        const int rr = q / kTile, kk = q % kTile;
+        sA[rr][kk] = (rr < rows && kk < K) ? A[(r0 + rr) * K + kk] : 0.f;
+    }
+    for (int q = threadIdx.x; q < K * H; q += blockDim.x) sW[q / H][q % H] = W[q];
+}
+
+__global__ void __launch_bounds__(kThreads) g_dense_fwd(int N, const float* __restrict__ X1, int K1,
+                                                        const float* __restrict__ W1, const float* __restrict__ X2,
+                                                        int K2, const float* __restrict__ W2,
+                                                        const float* __restrict__ b, float* __restrict__ Y, int relu) {
+    __shared__ float sA[kTile][kTile + 1];
+    __shared__ __align__(16) float sW[kTile][H];
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    for (long long r0 = (long long)blockIdx.x * kTile; r0 < N; r0 += (long long)gridDim.x * kTile) {
+        const int rows = (int)(N - r0 < kTile ? N - r0 : kTile);
+        float acc[4][4];
+        for (int j = 0; j < 4; ++j) {
+            const float bj = b[tx * 4 + j];
+            for (int i = 0; i < 4; ++i) acc[i][j] = bj;
+        }
+        for (int part = 0; part < 2; ++part) {
+            const float* X = part ? X2 : X1;
+            const float* W = part ? W2 : W1;
+            const int K = part ? K2 : K1;
+            if (!X) continue;
+            __syncthreads();
+            dense_stage(sA, sW, X, K, W, r0, rows);
+            __syncthreads();
+            for (int k = 0; k < K; ++k) {
+                const float4 w = *reinterpret_cast<const float4*>(&sW[k][tx * 4]);
+                for (int i = 0; i < 4; ++i) {
+                    const float x = sA[ty * 4 + i][k];
+                    acc[i][0] = fmaf(x, w.x, acc[i][0]);
+                    acc[i][1] = fmaf(x, w.y, acc[i][1]);
+                    acc[i][2] = fmaf(x, w.z, acc[i][2]);
+                    acc[i][3] = fmaf(x, w.w, acc[i][3]);
+                }
+            }
+        }
+        for (int i = 0; i < 4; ++i) {
+            const int rr = ty * 4 + i;
+            if (rr >= rows) continue;
+            float* y = Y + (r0 + rr) * H + tx * 4;
+            for (int j = 0; j < 4; ++j) y[j] = relu ? fmaxf(acc[i][j], 0.f) : acc[i][j];
+        }
     }
 }
 
@@ -101,15 +145,43 @@ __global__ void g_relu_bwd(long long count, const float* __restrict__ Y, float* 
 }
 
 // dX[N x K] (+)= dZ[N x H] W[K x H]^T
-__global__ void g_dense_bwd_x(int N, const float* __restrict__ dZ, const float* __restrict__ W, int K,
-                              float* __restrict__ dX, int accumulate) {
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)N * K;
-         t += (long long)gridDim.x * blockDim.x) {
-        const long long r = t / K;
-        const int k = (int)(t % K);
-        float acc = 0.f;
-        for (int c = 0; c < H; ++c) acc = fmaf(dZ[r * H + c], W[k * H + c], acc);
-        dX[t] = accumulate ? dX[t] + acc : acc;
+//
+// Tiled like g_dense_fwd: a 64-row tile of dZ and all of W in shared memory,
+// a 4 x 4 register block per thread (rows ty*4.., output columns tx*4..);
+// each output sums over c = 0..H-1 in order, as the one-thread-per-output form.
+__global__ void __launch_bounds__(kThreads) g_dense_bwd_x(int N, const float* __restrict__ dZ,
+                                                          const float* __restrict__ W, int K, float* __restrict__ dX,
+                                                          int accumulate) {
+    __shared__ float sZ[kTile][H + 1];
+    __shared__ float sW[kTile][H + 1];
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    for (int q = threadIdx.x; q < K * H; q += blockDim.x) sW[q / H][q % H] = W[q];
+    for (long long r0 = (long long)blockIdx.x * kTile; r0 < N; r0 += (long long)gridDim.x * kTile) {
+        const int rows = (int)(N - r0 < kTile ? N - r0 : kTile);
+        __syncthreads();
+        for (int q = threadIdx.x; q < kTile * H; q += blockDim.x) {
+            const int rr = q / H, cc = q % H;
+            sZ[rr][cc] = (rr < rows) ? dZ[(r0 + rr) * H + cc] : 0.f;
+        }
+        __syncthreads();
+        float acc[4][4] = {};
+        for (int c = 0; c < H; ++c) {
+            float w[4], z[4];
+            for (int j = 0; j < 4; ++j) w[j] = (tx * 4 + j < K) ? sW[tx * 4 + j][c] : 0.f;
+            for (int i = 0; i < 4; ++i) z[i] = sZ[ty * 4 + i][c];
+            for (int i = 0; i < 4; ++i)
+                for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(z[i], w[j], acc[i][j]);
+        }
+        for (int i = 0; i < 4; ++i) {
+            const int rr = ty * 4 + i;
+            if (rr >= rows) continue;
+            for (int j = 0; j < 4; ++j) {
+                const int k = tx * 4 + j;
+                if (k >= K) continue;
+                float* d = dX + (r0 + rr) * K + k;
+                *d = accumulate ? *d + acc[i][j] : acc[i][j];
+            }
+        }
     }
 }
 
@@ -266,6 +338,13 @@ __global__ void g_adam(long long count, float* __restrict__ p, const float* __re
 int grid_of(long long work) {
     long long b = (work + kThreads - 1) / kThreads;
     if (b > 4096) b = 4096;
+    return b < 1 ? 1 : (int)b;
+}
+
+// blocks of the tiled dense kernels: one per 64-row tile, at most four waves' worth
+int tile_grid(long long rows) {
+    long long b = (rows + kTile - 1) / kTile;
+    if (b > 148 * 8) b = 148 * 8;
     return b < 1 ? 1 : (int)b;
 }
 
@@ -464,20 +543,20 @@ int forward(mc_gnn* g, const Instance& I) {
     const float* P = g->params;
     const Layout& L = g->L;
     const int n = I.n, m = I.m;
-    g_dense_fwd<<<grid_of((long long)n * H), kThreads, 0, s>>>(n, I.Fv, FV, P + L.Wve, nullptr, 0, nullptr,
+    g_dense_fwd<<<tile_grid(n), kThreads, 0, s>>>(n, I.Fv, FV, P + L.Wve, nullptr, 0, nullptr,
                                                                P + L.bve, g->hv[0], 1);
-    g_dense_fwd<<<grid_of((long long)m * H), kThreads, 0, s>>>(m, I.Fc, FC, P + L.Wce, nullptr, 0, nullptr,
+    g_dense_fwd<<<tile_grid(m), kThreads, 0, s>>>(m, I.Fc, FC, P + L.Wce, nullptr, 0, nullptr,
                                                                P + L.bce, g->hc[0], 1);
     for (int r = 1; r <= g->rounds; ++r) {
         // constraints gather variables: agc_i = sum_j a_ij / |A_i| hv_j
         g_aggregate<<<grid_of((long long)m * 32), kThreads, 0, s>>>(m, I.rs, I.ci, I.rv, I.rinv, nullptr,
                                                                      g->hv[r - 1], g->agc[r], 0);
-        g_dense_fwd<<<grid_of((long long)m * H), kThreads, 0, s>>>(m, g->hc[r - 1], H, P + L.Wcs[r - 1], g->agc[r], H,
+        g_dense_fwd<<<tile_grid(m), kThreads, 0, s>>>(m, g->hc[r - 1], H, P + L.Wcs[r - 1], g->agc[r], H,
                                                                    P + L.Wcn[r - 1], P + L.bc[r - 1], g->hc[r], 1);
         // variables gather constraints: agv_j = sum_i a_ij / |A_j| hc_i
         g_aggregate<<<grid_of((long long)n * 32), kThreads, 0, s>>>(n, I.cs, I.ri, I.cv, I.cinv, nullptr,
                                                                      g->hc[r], g->agv[r], 0);
-        g_dense_fwd<<<grid_of((long long)n * H), kThreads, 0, s>>>(n, g->hv[r - 1], H, P + L.Wvs[r - 1], g->agv[r], H,
+        g_dense_fwd<<<tile_grid(n), kThreads, 0, s>>>(n, g->hv[r - 1], H, P + L.Wvs[r - 1], g->agv[r], H,
                                                                    P + L.Wvn[r - 1], P + L.bv[r - 1], g->hv[r], 1);
     }
     const int R = g->rounds;
@@ -589,8 +668,8 @@ int loss_and_grad(mc_gnn* g, const Instance& I, double target_logw, double* loss
         g_relu_bwd<<<grid_of((long long)n * H), kThreads, 0, s>>>((long long)n * H, g->hv[r], g->dhv);
         GTRY(weight_grad(g, n, g->hv[r - 1], H, g->dhv, L.Wvs[r - 1], L.bv[r - 1]));
         GTRY(weight_grad(g, n, g->agv[r], H, g->dhv, L.Wvn[r - 1], -1));
-        g_dense_bwd_x<<<grid_of((long long)n * H), kThreads, 0, s>>>(n, g->dhv, P + L.Wvs[r - 1], H, g->dhv2, 0);
-        g_dense_bwd_x<<<grid_of((long long)n * H), kThreads, 0, s>>>(n, g->dhv, P + L.Wvn[r - 1], H, g->dag, 0);
+        g_dense_bwd_x<<<tile_grid(n), kThreads, 0, s>>>(n, g->dhv, P + L.Wvs[r - 1], H, g->dhv2, 0);
+        g_dense_bwd_x<<<tile_grid(n), kThreads, 0, s>>>(n, g->dhv, P + L.Wvn[r - 1], H, g->dag, 0);
         // agv[r]_j = sum_i a_ij cinv_j hc[r]_i  ->  d hc[r]_i += sum_j a_ij cinv_j d agv_j (CSR)
         g_aggregate<<<grid_of((long long)m * 32), kThreads, 0, s>>>(m, I.rs, I.ci, I.rv, nullptr, I.cinv, g->dag,
                                                                      g->dhc, 1);
@@ -598,8 +677,8 @@ int loss_and_grad(mc_gnn* g, const Instance& I, double target_logw, double* loss
         g_relu_bwd<<<grid_of((long long)m * H), kThreads, 0, s>>>((long long)m * H, g->hc[r], g->dhc);
         GTRY(weight_grad(g, m, g->hc[r - 1], H, g->dhc, L.Wcs[r - 1], L.bc[r - 1]));
         GTRY(weight_grad(g, m, g->agc[r], H, g->dhc, L.Wcn[r - 1], -1));
-        g_dense_bwd_x<<<grid_of((long long)m * H), kThreads, 0, s>>>(m, g->dhc, P + L.Wcs[r - 1], H, g->dhc2, 0);
-        g_dense_bwd_x<<<grid_of((long long)m * H), kThreads, 0, s>>>(m, g->dhc, P + L.Wcn[r - 1], H, g->dag, 0);
+        g_dense_bwd_x<<<tile_grid(m), kThreads, 0, s>>>(m, g->dhc, P + L.Wcs[r - 1], H, g->dhc2, 0);
+        g_dense_bwd_x<<<tile_grid(m), kThreads, 0, s>>>(m, g->dhc, P + L.Wcn[r - 1], H, g->dag, 0);
         // agc[r]_i = sum_j a_ij rinv_i hv[r-1]_j  ->  d hv[r-1]_j += sum_i a_ij rinv_i d agc_i (CSC)
         g_aggregate<<<grid_of((long long)n * 32), kThreads, 0, s>>>(n, I.cs, I.ri, I.cv, nullptr, I.rinv, g->dag,
                                                                      g->dhv2, 1);
