@@ -483,10 +483,16 @@ int mc_lp_file_read(const char* path, mc_lp* lp);
  * about 8 MiB that every GPU loading the library holds until exit.
  * Limits: m + n <= 1,048,576, else MC_ERR_RESOURCE_LIMIT (nothing launched).
  * Runs on the current device and `stream` (a cudaStream_t, NULL = default
- * stream); *iterations_executed (may be NULL) is read back with a stream
- * synchronisation.  The first call on a device looks the array up with
- * cudaGetSymbolAddress: make it before any stream capture.  Calls share the
- * array, so calls that can overlap on the GPU race and must be serialised.
+ * stream).  With iterations_executed non-NULL the call reads the pass count
+ * back with a stream synchronisation and reports errors of its kernels; with
+ * it NULL the call returns once its work is enqueued, asynchronously on
+ * `stream`, and errors that arise while the kernels run surface only in the
+ * caller's own later checks of that stream.  The first call on a device looks
+ * the array up with cudaGetSymbolAddress and keeps the address for the life
+ * of the process: make that call before any stream capture, and do not call
+ * on a device after cudaDeviceReset (the kept address belongs to the old
+ * context).  Calls share the array, so calls that can overlap on the GPU race
+ * and must be serialised.
  */
 int mc_ruiz_equilibrate_noalloc(int32_t m, int32_t n, int64_t nnz, const int32_t* col_start,
                                 const int32_t* row_index, double* csc_value,

@@ -18,7 +18,11 @@
 //   * The first call on a device looks up the array's device address with
 //     cudaGetSymbolAddress (host code cannot use the array's name as a device
 //     pointer) and caches it per device; make that first call before any
-//     stream capture begins.
+//     stream capture begins.  A cudaDeviceReset ends the context the cached
+//     address belongs to, so the entry point must not be called on that
+//     device afterwards.
+//   * Without iterations_executed the call is asynchronous on its stream and
+//     does not see errors raised while its kernels run.
 //   * All calls share the one array: calls that may overlap on the GPU (on
 //     different streams, or from different host threads) race on it and must
 //     be serialised by the caller.  Each call re-initialises the parts that
