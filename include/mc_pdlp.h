@@ -183,8 +183,10 @@ typedef struct mc_pdlp_result {
  *                     U = sum_i (y_i > 0 ? y_i row_upper[i] : y_i row_lower[i])
  *                   all finite and L > U; for every x in the box
  *                   L <= g.x = y.(A x) <= U would hold if x were feasible.
- *                   Found by the restart checks: the dual average of a
- *                   primal infeasible LP diverges along such a ray. */
+ *                   Found by the restart checks: the change of the dual
+ *                   average between two checks, with its components on
+ *                   one-sided rows projected to the allowed sign -- the dual
+ *                   iterates of a primal infeasible LP diverge along a ray. */
 enum {
     MC_CERT_NONE = 0,
     MC_CERT_CROSSED_BOUNDS = 1,

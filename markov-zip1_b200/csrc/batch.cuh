@@ -338,6 +338,7 @@ int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o,
     const size_t o_off = L.add<double>(2LL * count);
     const size_t o_flags = L.add<int>(count);
     const size_t o_cert = L.add<int>(2LL * count);
+    const size_t o_yprev = L.add<double>(m), o_dray = L.add<double>(m);
     bool any_warm = false;
     for (int b = 0; b < count; ++b)
         any_warm = any_warm || (x0 && x0[b] && lps[b].num_cols > 0) || (y0 && y0[b] && lps[b].num_rows > 0);
@@ -479,6 +480,7 @@ int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o,
     CU(cudaMemsetAsync(rv + nnz, 0, sizeof(double) * 16, s));
     CU(cudaMemsetAsync(flags, 0, sizeof(int) * count, s));
     CU(cudaMemsetAsync(cert_idx, 0x7f, sizeof(int) * 2 * (size_t)count, s));  // "none" above any index
+    CU(cudaMemsetAsync(at(o_dray), 0, sizeof(double) * (size_t)m, s));
     CU(cudaMemsetAsync(st, 0, sizeof(DevState) * (count + 1), s));
     CU(cudaEventRecord(ctx.ev_b, s));
     int bad = 0;
@@ -492,6 +494,8 @@ int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o,
     B.offset = offsets;
     B.flags = flags;
     B.cert_idx = cert_idx;
+    B.y_prev = static_cast<double*>(at(o_yprev));
+    B.dray = static_cast<double*>(at(o_dray));
     B.nlp = count;
     B.warm = warm;
     B.warm_x = warm_x;

@@ -46,6 +46,8 @@ struct BatchRefs {
     int* flags;                // [nlp] setup certificates: 1 crossed bounds, 2 row activity
     int* cert_idx;             // [2 nlp] lowest crossed column, lowest failing row of each LP
                                // (LP-local indices; INT_MAX if none)
+    double* y_prev;            // [m] dual average at the previous check (scaled; the start at setup)
+    double* dray;              // [m] the ray candidate of the current check (scaled)
     const int* warm;           // [nlp] starting point given: 1 primal, 2 dual (NULL: none)
     const double* warm_x;      // [n] packed starting primal (original space)
     const double* warm_y;      // [m] packed starting dual
@@ -70,19 +72,33 @@ struct BatchRefs {
          base_ < tl1_ && ((LINE = base_ + (int)(threadIdx.x / G)), true); base_ += kBlock / G)     \
         if (const bool VALID = LINE < tl1_; true)
 
-// The Farkas test of the dual average, evaluated in the residual pass on the
-// unscaled y = y_avg and g = A^T y (the residual pass's own product, without
-// c).  For any x in the variable box that met the rows,
-//     L = sum_j (g_j > 0 ? g_j lo_j : g_j hi_j) <= g.x = y.(A x) <= U,
-//     U = sum_i (y_i > 0 ? y_i hi_i : y_i lo_i) = -(the row part of the dual
-//         objective, RowTerms::dsum),
-// so L > U proves the LP infeasible.  The dual update's projection keeps the
-// signs of y consistent with the finite row bounds; a nonzero term meeting an
-// infinite bound makes the side infinite and is counted instead.  The scales
-// bound the rounding of both sums (|bound| times sum |a y| per column, |y
-// bound| per row), so a margin of 1e-9 of them cannot come from rounding.
+// The Farkas test, evaluated in the residual pass on a dual ray candidate d:
+// the change of the dual average since the previous check (unscaled), with
+// its components on one-sided rows projected to the sign the finite bound
+// allows (and zeroed on free rows).  For a primal infeasible LP the dual
+// iterates diverge along a ray, so these differences point along it while
+// the bounded part of the average cancels.  With g = A^T d,
+//     L = sum_j (g_j > 0 ? g_j lo_j : g_j hi_j) <= g.x = d.(A x) <= U,
+//     U = sum_i (d_i > 0 ? d_i hi_i : d_i lo_i)
+// would hold for any x in the variable box that met the rows, so L > U proves
+// the LP infeasible.  A nonzero g_j meeting an infinite bound makes L = -inf
+// and is counted instead.  The scales bound the rounding of both sums (|bound|
+// times sum |a d| per column, |d bound| per row), so a margin of 1e-9 of them
+// cannot come from rounding.
 struct RayTerms {
-    double l = 0.0, cscale = 0.0, cinf = 0.0, rscale = 0.0, rinf = 0.0;
+    double l = 0.0, cscale = 0.0, cinf = 0.0, u = 0.0, rscale = 0.0, rinf = 0.0;
+    // the candidate of row i (scaled units) from the current and the previous
+    // check's dual averages; the current one becomes the previous
+    __device__ __forceinline__ static double candidate(const Original& O, int i, double y_now, double* y_prev) {
+        double d = y_now - *y_prev;
+        *y_prev = y_now;
+        const double lo = O.blo[i], hi = O.bhi[i];
+        const bool lo_inf = lo <= -1e299, hi_inf = hi >= 1e299;
+        if (lo_inf && hi_inf) d = 0.0;
+        else if (lo_inf) d = maxv(d, 0.0);
+        else if (hi_inf) d = minv(d, 0.0);
+        return d;
+    }
     __device__ __forceinline__ void add_col(const Original& O, int j, double s, double s_abs) {
         add_col_b(O, j, s, s_abs, O.lo[j], O.hi[j]);
     }
@@ -100,12 +116,17 @@ struct RayTerms {
             }
         }
     }
-    __device__ __forceinline__ void add_row(const Original& O, int i, double y_scaled) {
-        const double yu = __dmul_rn(y_scaled, O.row_scale[i]);
-        if (yu == 0.0) return;
-        const double bnd = (yu > 0.0) ? O.bhi[i] : O.blo[i];
-        if (fabs(bnd) >= 1e299) rinf += 1.0;
-        else rscale += fabs(yu * bnd);
+    __device__ __forceinline__ void add_row(const Original& O, int i, double d_scaled) {
+        const double du = __dmul_rn(d_scaled, O.row_scale[i]);
+        if (du == 0.0) return;
+        const double bnd = (du > 0.0) ? O.bhi[i] : O.blo[i];
+        if (fabs(bnd) >= 1e299) {
+            rinf += 1.0;
+        } else {
+            const double t = __dmul_rn(du, bnd);
+            u += t;
+            rscale += fabs(t);
+        }
     }
     __device__ __forceinline__ void store_cols(double* partials, double* scratch, int t) {
         l = block_reduce(l, scratch, OpSum());
@@ -118,9 +139,11 @@ struct RayTerms {
         }
     }
     __device__ __forceinline__ void store_rows(double* partials, double* scratch, int t) {
+        u = block_reduce(u, scratch, OpSum());
         rscale = block_reduce(rscale, scratch, OpSum());
         rinf = block_reduce(rinf, scratch, OpSum());
         if (threadIdx.x == 0) {
+            partials[SLOT_RAY_U * kMaxTiles + t] = u;
             partials[SLOT_RAY_RSCALE * kMaxTiles + t] = rscale;
             partials[SLOT_RAY_RINF * kMaxTiles + t] = rinf;
         }
@@ -257,7 +280,9 @@ __global__ void __launch_bounds__(kBlock) kb_residual_rows(Iterates<double> P, O
             s = group_sum<G>(s);
             if (valid && sub == 0) {
                 acc.add(O, i, s, P.y_avg[i]);
-                ray.add_row(O, i, P.y_avg[i]);
+                const double d = RayTerms::candidate(O, i, P.y_avg[i], B.y_prev + i);
+                B.dray[i] = d;
+                ray.add_row(O, i, d);
             }
         }
         acc.vmax = block_reduce(acc.vmax, scratch, OpMax());
@@ -279,20 +304,23 @@ __global__ void __launch_bounds__(kBlock) kb_residual_cols(Iterates<double> P, O
         ColTerms acc;
         RayTerms ray;
         MC_TILE_LINES(B.cols, t, j, valid, sub) {
-            double s = 0.0, sa = 0.0;
+            double s = 0.0, sd = 0.0, sa = 0.0;
             if (valid) {
                 const int b = P.csc_start[j], e = P.csc_start[j + 1];
                 for (int p = b + sub; p < e; p += G) {
-                    const double a = P.csc_val[p], yv = P.y_avg[P.csc_row[p]];
-                    s = fma(a, yv, s);
-                    sa = fma(fabs(a), fabs(yv), sa);
+                    const int ii = P.csc_row[p];
+                    const double a = P.csc_val[p], dv = B.dray[ii];
+                    s = fma(a, P.y_avg[ii], s);
+                    sd = fma(a, dv, sd);
+                    sa = fma(fabs(a), fabs(dv), sa);
                 }
             }
             s = group_sum<G>(s);
+            sd = group_sum<G>(sd);
             sa = group_sum<G>(sa);
             if (valid && sub == 0) {
                 acc.add(O, j, s, P.x_avg[j]);
-                ray.add_col(O, j, s, sa);
+                ray.add_col(O, j, sd, sa);
             }
         }
         acc.vmax = block_reduce(acc.vmax, scratch, OpMax());
@@ -334,10 +362,11 @@ __global__ void kb_finalize(const double* __restrict__ partials, BatchRefs B, lo
     const double ray_ci = reduce_partials(partials + SLOT_RAY_CINF * kMaxTiles + c0, nc, scratch, OpSum());
     const double ray_rs = reduce_partials(partials + SLOT_RAY_RSCALE * kMaxTiles + r0, nr, scratch, OpSum());
     const double ray_ri = reduce_partials(partials + SLOT_RAY_RINF * kMaxTiles + r0, nr, scratch, OpSum());
+    const double ray_u = reduce_partials(partials + SLOT_RAY_U * kMaxTiles + r0, nr, scratch, OpSum());
     if (threadIdx.x != 0) return;
     const double offset = B.offset[lp];
-    // the Farkas test of the dual average (RayTerms): U = -row_dobj
-    const double margin = ray_l + row_dobj;
+    // the Farkas test of the ray candidate (RayTerms)
+    const double margin = ray_l - ray_u;
     const bool farkas = ray_ci == 0.0 && ray_ri == 0.0 && margin > 0.0 && margin > 1e-9 * (ray_cs + ray_rs);
     const double primal = maxv(row_max, col_max);
     const double dual = sqrt(col_dres) / st->c_scale;
@@ -561,6 +590,7 @@ __global__ void kb_setup_rows(const int* __restrict__ row_start, const int* __re
         const double y0 = (B.warm && (B.warm[lp] & 2)) ? __dmul_rn(B.warm_y[i], 1.0 / s) : 0.0;
         P.y[i] = y0;
         P.y_avg[i] = y0;
+        B.y_prev[i] = y0;
     }
     if (infeasible) atomicOr(B.flags + lp, 2);
     bmax = block_reduce(bmax, scratch, OpMax());
@@ -619,8 +649,12 @@ __global__ void kb_unscale_out(const double* __restrict__ x_avg, const float* __
     const bool col = blockIdx.x < (unsigned)B.cols.ntiles;
     const int t = col ? blockIdx.x : blockIdx.x - B.cols.ntiles;
     const TileTable& T = col ? B.cols : B.rows;
+    // an LP proven infeasible by a dual ray returns the ray as its dual
+    const DevState& S = B.st[T.lp[t]];
+    const bool ray = S.status == 2 && S.cert == MC_CERT_DUAL_RAY;
     for (int l = T.l0[t] + threadIdx.x; l < T.l1[t]; l += blockDim.x) {
         if (col) x_out[l] = __dmul_rn(dx_avg ? x_avg[l] + (double)dx_avg[l] : x_avg[l], col_scale[l]);
+        else if (ray) y_out[l] = __dmul_rn(B.dray[l], row_scale[l]);
         else y_out[l] = __dmul_rn(dy_avg ? y_avg[l] + (double)dy_avg[l] : y_avg[l], row_scale[l]);
     }
 }
@@ -776,7 +810,9 @@ __global__ void __launch_bounds__(kBlock) kb_residual_rows_mx(Iterates<float> P,
                 M.ax_full[i] = s;
                 const double yv = M.y_hat[i] + (double)P.y_avg[i];
                 acc.add(O, i, s, yv);
-                ray.add_row(O, i, yv);
+                const double d = RayTerms::candidate(O, i, yv, B.y_prev + i);
+                B.dray[i] = d;
+                ray.add_row(O, i, d);
             }
         }
         acc.vmax = block_reduce(acc.vmax, scratch, OpMax());
@@ -799,22 +835,24 @@ __global__ void __launch_bounds__(kBlock) kb_residual_cols_mx(Iterates<float> P,
         ColTerms acc;
         RayTerms ray;
         MC_TILE_LINES(B.cols, t, j, valid, sub) {
-            double s = 0.0, sa = 0.0;
+            double s = 0.0, sd = 0.0, sa = 0.0;
             if (valid) {
                 const int b = P.csc_start[j], e = P.csc_start[j + 1];
                 for (int p = b + sub; p < e; p += G) {
                     const int ii = P.csc_row[p];
-                    const double a = M.csc_val64[p], yv = M.y_hat[ii] + (double)P.y_avg[ii];
-                    s = fma(a, yv, s);
-                    sa = fma(fabs(a), fabs(yv), sa);
+                    const double a = M.csc_val64[p], dv = B.dray[ii];
+                    s = fma(a, M.y_hat[ii] + (double)P.y_avg[ii], s);
+                    sd = fma(a, dv, sd);
+                    sa = fma(fabs(a), fabs(dv), sa);
                 }
             }
             s = group_sum<G>(s);
+            sd = group_sum<G>(sd);
             sa = group_sum<G>(sa);
             if (valid && sub == 0) {
                 M.aty_full[j] = s;
                 acc.add(O, j, s, M.x_hat[j] + (double)P.x_avg[j]);
-                ray.add_col(O, j, s, sa);
+                ray.add_col(O, j, sd, sa);
             }
         }
         acc.vmax = block_reduce(acc.vmax, scratch, OpMax());

@@ -31,13 +31,14 @@ enum PartialSlot : int {
     SLOT_B = 9,
     SLOT_C = 10,
     SLOT_NAN = 11,      // count of non-finite values seen in a residual pass
-    // batch residual pass: the Farkas test of the dual average (batch_kernels.cuh)
-    SLOT_RAY_L = 12,       // sum_j (g_j > 0 ? g_j lo_j : g_j hi_j), g = A^T y_avg     (columns)
-    SLOT_RAY_CSCALE = 13,  // sum_j |bound_j| sum_i |a_ij y_i|: rounding scale        (columns)
+    // batch residual pass: the Farkas test of the dual ray candidate d (batch_kernels.cuh)
+    SLOT_RAY_L = 12,       // sum_j (g_j > 0 ? g_j lo_j : g_j hi_j), g = A^T d          (columns)
+    SLOT_RAY_CSCALE = 13,  // sum_j |bound_j| sum_i |a_ij d_i|: rounding scale        (columns)
     SLOT_RAY_CINF = 14,    // count of nonzero g_j meeting an infinite bound           (columns)
-    SLOT_RAY_RSCALE = 15,  // sum_i |y_i bound_i|                                      (rows)
-    SLOT_RAY_RINF = 16,    // count of nonzero y_i meeting an infinite bound           (rows)
-    NUM_SLOTS = 17
+    SLOT_RAY_RSCALE = 15,  // sum_i |d_i bound_i|                                      (rows)
+    SLOT_RAY_RINF = 16,    // count of nonzero d_i meeting an infinite bound           (rows)
+    SLOT_RAY_U = 17,       // sum_i (d_i > 0 ? d_i hi_i : d_i lo_i)                    (rows)
+    NUM_SLOTS = 18
 };
 
 // Scalars of one solve, resident in device memory so that whole restart
@@ -112,24 +113,6 @@ __device__ __forceinline__ void st_keep(float* a, float v, unsigned long long po
 }
 template <class T>
 __device__ __forceinline__ T ld_stream(const T* a) { return __ldcs(a); }
-// 16-byte streaming loads of four indices / two doubles / four floats (the
-// address must be 16-byte aligned)
-__device__ __forceinline__ int4 ld_stream4(const int* a) { return __ldcs(reinterpret_cast<const int4*>(a)); }
-__device__ __forceinline__ void ld_stream_quad(const double* a, double& v0, double& v1, double& v2, double& v3) {
-    const double2 lo = __ldcs(reinterpret_cast<const double2*>(a));
-    const double2 hi = __ldcs(reinterpret_cast<const double2*>(a + 2));
-    v0 = lo.x;
-    v1 = lo.y;
-    v2 = hi.x;
-    v3 = hi.y;
-}
-__device__ __forceinline__ void ld_stream_quad(const float* a, float& v0, float& v1, float& v2, float& v3) {
-    const float4 q = __ldcs(reinterpret_cast<const float4*>(a));
-    v0 = q.x;
-    v1 = q.y;
-    v2 = q.z;
-    v3 = q.w;
-}
 template <class T>
 __device__ __forceinline__ void st_stream(T* a, T v) { __stcs(a, v); }
 

@@ -82,40 +82,14 @@ template <> __device__ __forceinline__ float div_rn(float a, float b) { return _
 // Dot of line `j` of a compressed matrix with vector v, G lanes per line,
 // four independent gathers in flight per lane per step.  The matrix is
 // streamed (evict-first); v is gathered with the keep policy.
-#if MC_LINE_DOT_VEC
-// Vector form: the line's entries are taken in aligned quads (4-entry groups
-// from the array base), one 16-byte index load and one 32-byte value load
-// (two 16-byte halves) per quad and lane, so a lane group reads whole
-// contiguous 16-byte pieces; the head before the first aligned quad is read
-// entry by entry.  Entries of a quad beyond the line are masked (their loads
-// stay inside the array's 16-entry padding or the next lines).
+// (Loading the matrix in aligned 16-byte quads per lane instead was measured
+// on B200 at the 40M-nonzero LP: no faster -- 0.248 / 0.245 ms per primal /
+// dual launch against 0.244 / 0.245 -- as the streamed lines already merge in
+// L1 between a lane group's unrolled loads.)
 template <int G, class T>
 __device__ __forceinline__ T line_dot(const int* __restrict__ start, const int* __restrict__ idx,
                                       const T* __restrict__ val, const T* __restrict__ v, int j,
                                       bool valid, int sub, unsigned long long pol) {
-    T s0 = T(0), s1 = T(0), s2 = T(0), s3 = T(0);
-    if (valid) {
-        const int b = __ldg(start + j), e = __ldg(start + j + 1);
-        const int ab = min((b + 3) & ~3, e);
-        for (int p = b + sub; p < ab; p += G) s3 = fma(ld_stream(val + p), ld_keep(v + ld_stream(idx + p), pol), s3);
-        for (int q = ab + 4 * sub; q < e; q += 4 * G) {
-            const int4 I = ld_stream4(idx + q);
-            T a0, a1, a2, a3;
-            ld_stream_quad(val + q, a0, a1, a2, a3);
-            s0 = fma(a0, ld_keep(v + I.x, pol), s0);
-            if (q + 1 < e) s1 = fma(a1, ld_keep(v + I.y, pol), s1);
-            if (q + 2 < e) s2 = fma(a2, ld_keep(v + I.z, pol), s2);
-            if (q + 3 < e) s3 = fma(a3, ld_keep(v + I.w, pol), s3);
-        }
-    }
-    return group_sum<G>((s0 + s1) + (s2 + s3));
-}
-#endif
-// Scalar form (no alignment or padding needed: used on caller arrays too).
-template <int G, class T>
-__device__ __forceinline__ T line_dot_scalar(const int* __restrict__ start, const int* __restrict__ idx,
-                                             const T* __restrict__ val, const T* __restrict__ v, int j,
-                                             bool valid, int sub, unsigned long long pol) {
     T s0 = T(0), s1 = T(0), s2 = T(0), s3 = T(0);
     if (valid) {
         const int b = __ldg(start + j), e = __ldg(start + j + 1);
@@ -134,14 +108,6 @@ __device__ __forceinline__ T line_dot_scalar(const int* __restrict__ start, cons
     }
     return group_sum<G>((s0 + s1) + (s2 + s3));
 }
-#if !MC_LINE_DOT_VEC
-template <int G, class T>
-__device__ __forceinline__ T line_dot(const int* __restrict__ start, const int* __restrict__ idx,
-                                      const T* __restrict__ val, const T* __restrict__ v, int j,
-                                      bool valid, int sub, unsigned long long pol) {
-    return line_dot_scalar<G>(start, idx, val, v, j, valid, sub, pol);
-}
-#endif
 
 // Two dots of the same line against an interleaved pair vector vw[2c] = v_c,
 // vw[2c+1] = w_c (A x-bar and A dx on step-size iterations): one gather per
@@ -191,7 +157,7 @@ __global__ void __launch_bounds__(kBlock) k_spmv(int rows, const int* __restrict
     for (long long t = warp; t * LPW < rows; t += nwarps) {
         const int i = (int)(t * LPW) + slot;
         const bool valid = i < rows;
-        const T s = line_dot_scalar<G>(start, idx, val, x, i, valid, sub, pol);
+        const T s = line_dot<G>(start, idx, val, x, i, valid, sub, pol);
         if (valid && sub == 0) y[i] = s;
     }
 }

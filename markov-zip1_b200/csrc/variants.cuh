@@ -20,7 +20,7 @@
 // one partial per variant and a per-variant kernel sums them in a fixed
 // order, so results are run-to-run deterministic.  Infeasible variants are
 // certified as in the packed batch (crossed bounds, row activity, and the
-// Farkas test of the dual average at every restart check).
+// Farkas test of the dual ray candidate at every restart check).
 #pragma once
 
 #include "batch.cuh"
@@ -61,6 +61,8 @@ struct VarRefs {
     double* y;             // [m Kp]
     double* ya;
     double* axb;           // [m Kp] A x-bar of a step-size iteration
+    double* y_prev;        // [m Kp] dual average at the previous check (the start at setup)
+    double* dray;          // [m Kp] the dual ray candidate of the current check
     double* partials;      // [NUM_SLOTS Kp nb]
     int* flags;            // [K] setup certificates: 1 crossed bounds, 2 row activity
     int* cert_idx;         // [2K] lowest crossed column, lowest failing row (INT_MAX if none)
@@ -275,20 +277,25 @@ __global__ void __launch_bounds__(kBlock) kv_residual_rows(VarBase Bs, VarRefs V
     MC_VARIANT_LINES(i, Bs.m) {
         const double s = variant_dot(Bs.rs, Bs.ci, Bs.rv, V.xa, V.Kp, i, k, live, pol);
         if (live) {
-            const double yv = V.ya[(size_t)i * V.Kp + k];
+            const size_t q = (size_t)i * V.Kp + k;
+            const double yv = V.ya[q];
             acc.add(O, (int)i, s, yv);
-            ray.add_row(O, (int)i, yv);
+            const double d = RayTerms::candidate(O, (int)i, yv, V.y_prev + q);
+            V.dray[q] = d;
+            ray.add_row(O, (int)i, d);
         }
     }
     const double vmax = lanes_reduce(acc.vmax, sm, OpMax());
     const double dsum = lanes_reduce(acc.dsum, sm, OpSum());
     const double bad = lanes_reduce(acc.bad, sm, OpSum());
+    const double ru = lanes_reduce(ray.u, sm, OpSum());
     const double rsc = lanes_reduce(ray.rscale, sm, OpSum());
     const double rinf = lanes_reduce(ray.rinf, sm, OpSum());
     if ((threadIdx.x >> 5) == 0 && k < V.K) {
         var_partial(V, SLOT_ROW_MAX, k)[blockIdx.x] = vmax;
         var_partial(V, SLOT_ROW_DOBJ, k)[blockIdx.x] = dsum;
         var_partial(V, SLOT_NAN, k)[blockIdx.x] = bad;
+        var_partial(V, SLOT_RAY_U, k)[blockIdx.x] = ru;
         var_partial(V, SLOT_RAY_RSCALE, k)[blockIdx.x] = rsc;
         var_partial(V, SLOT_RAY_RINF, k)[blockIdx.x] = rinf;
     }
@@ -302,17 +309,19 @@ __global__ void __launch_bounds__(kBlock) kv_residual_cols(VarBase Bs, VarRefs V
     RayTerms ray;
     MC_VARIANT_LINES(j, Bs.n) {
         const int b = __ldg(Bs.cs + j), e = __ldg(Bs.cs + j + 1);
-        double s = 0.0, sa = 0.0;
+        double s = 0.0, sd = 0.0, sa = 0.0;
         if (live) {
             for (int p = b; p < e; ++p) {
                 const double a = __ldg(Bs.cv + p);
-                const double yv = ld_keep(V.ya + (size_t)__ldg(Bs.ri + p) * V.Kp + k, pol);
-                s = fma(a, yv, s);
-                sa = fma(fabs(a), fabs(yv), sa);
+                const size_t qi = (size_t)__ldg(Bs.ri + p) * V.Kp + k;
+                const double dv = V.dray[qi];
+                s = fma(a, ld_keep(V.ya + qi, pol), s);
+                sd = fma(a, dv, sd);
+                sa = fma(fabs(a), fabs(dv), sa);
             }
             const size_t q = (size_t)j * V.Kp + k;
             acc.add_b(O, (int)j, s, V.xa[q], V.olo[q], V.ohi[q]);
-            ray.add_col_b(O, (int)j, s, sa, V.olo[q], V.ohi[q]);
+            ray.add_col_b(O, (int)j, sd, sa, V.olo[q], V.ohi[q]);
         }
     }
     const double vmax = lanes_reduce(acc.vmax, sm, OpMax());
@@ -356,6 +365,7 @@ __global__ void kv_finalize(VarRefs V, double offset, long long span, int final_
     const double ray_ci = reduce_partials(var_partial(V, SLOT_RAY_CINF, k), nb, scratch, OpSum());
     const double ray_rs = reduce_partials(var_partial(V, SLOT_RAY_RSCALE, k), nb, scratch, OpSum());
     const double ray_ri = reduce_partials(var_partial(V, SLOT_RAY_RINF, k), nb, scratch, OpSum());
+    const double ray_u = reduce_partials(var_partial(V, SLOT_RAY_U, k), nb, scratch, OpSum());
     if (threadIdx.x != 0) return;
     const double primal = maxv(row_max, col_max);
     const double dual = sqrt(col_dres) / st->c_scale;
@@ -363,7 +373,7 @@ __global__ void kv_finalize(VarRefs V, double offset, long long span, int final_
     const double dobj = (offset + row_dobj) + col_dobj;
     const double gap = fabs(pobj - dobj) / (1.0 + fabs(pobj) + fabs(dobj));
     const double score = maxv(maxv(primal, dual), gap);
-    const double margin = ray_l + row_dobj;
+    const double margin = ray_l - ray_u;
     const bool farkas = ray_ci == 0.0 && ray_ri == 0.0 && margin > 0.0 && margin > 1e-9 * (ray_cs + ray_rs);
     st->primal_infeas = primal;
     st->dual_infeas = dual;
@@ -499,7 +509,7 @@ __global__ void __launch_bounds__(kBlock) kv_setup_rows(VarBase Bs, VarRefs V, c
     MC_VARIANT_LINES(i, Bs.m) {
         const size_t q = (size_t)i * V.Kp + k;
         if (!real) {
-            V.y[q] = V.ya[q] = V.axb[q] = 0.0;
+            V.y[q] = V.ya[q] = V.axb[q] = V.y_prev[q] = V.dray[q] = 0.0;
             continue;
         }
         const double s = row_scale[i];
@@ -526,6 +536,8 @@ __global__ void __launch_bounds__(kBlock) kv_setup_rows(VarBase Bs, VarRefs V, c
         V.y[q] = y0;
         V.ya[q] = y0;
         V.axb[q] = 0.0;
+        V.y_prev[q] = y0;
+        V.dray[q] = 0.0;
     }
 }
 
@@ -558,12 +570,15 @@ __global__ void __launch_bounds__(kBlock) kv_unscale_out(VarBase Bs, VarRefs V, 
                                                          double* __restrict__ yo) {
     const int k = blockIdx.y * 32 + (threadIdx.x & 31);
     if (k >= V.K) return;
+    // a variant proven infeasible by a dual ray returns the ray as its dual
+    const bool ray = V.st[k].status == 2 && V.st[k].cert == MC_CERT_DUAL_RAY;
+    const double* yv = ray ? V.dray : V.ya;
     MC_VARIANT_LINES(l, (long long)Bs.n + Bs.m) {
         if (l < Bs.n) {
             xo[(size_t)k * Bs.n + l] = __dmul_rn(V.xa[(size_t)l * V.Kp + k], col_scale[l]);
         } else {
             const long long i = l - Bs.n;
-            yo[(size_t)k * Bs.m + i] = __dmul_rn(V.ya[(size_t)i * V.Kp + k], row_scale[i]);
+            yo[(size_t)k * Bs.m + i] = __dmul_rn(yv[(size_t)i * V.Kp + k], row_scale[i]);
         }
     }
 }
@@ -694,7 +709,7 @@ int solve_variants(Ctx& ctx, const mc_lp* base, int count, const double* const* 
     const size_t o_part1 = L.add<double>((long long)NUM_SLOTS * kMaxPartials);
     const size_t o_state = L.add<DevState>(count + 2);
     const long long nk = (long long)n * Kp, mk = (long long)m * Kp;
-    size_t o_vn[7], o_vm[3];
+    size_t o_vn[7], o_vm[5];
     for (auto& v : o_vn) v = L.add<double>(nk);
     const size_t o_vxdx = L.add<double>(2 * nk);
     for (auto& v : o_vm) v = L.add<double>(mk);
@@ -827,6 +842,8 @@ int solve_variants(Ctx& ctx, const mc_lp* base, int count, const double* const* 
     V.y = static_cast<double*>(at(o_vm[0]));
     V.ya = static_cast<double*>(at(o_vm[1]));
     V.axb = static_cast<double*>(at(o_vm[2]));
+    V.y_prev = static_cast<double*>(at(o_vm[3]));
+    V.dray = static_cast<double*>(at(o_vm[4]));
     V.partials = static_cast<double*>(at(o_vpart));
     V.flags = static_cast<int*>(at(o_flags));
     V.cert_idx = static_cast<int*>(at(o_cert));

@@ -195,7 +195,7 @@ def start_scores(ctx: Context, models: list, options: PdlpOptions, starts_x=None
 
 
 def evaluate_batched(ctx: Context, net: WarmStartNet, models: list, options: PdlpOptions,
-                     batch: int = 256) -> list:
+                     batch: int = 256, forced: bool = True) -> list:
     """Cold against learned warm starts on held-out LPs, in batched solves.
 
     Per LP: the cold solve; the prediction's start score against the cold
@@ -220,9 +220,9 @@ def evaluate_batched(ctx: Context, net: WarmStartNet, models: list, options: Pdl
                                initial_dual=[y if u else None for y, u in zip(py, use)])
         t_warm = _t.perf_counter() - t
         t = _t.perf_counter()
-        forced = ctx.solve_batch(chunk, options, initial_primal=px, initial_dual=py)
-        t_forced = _t.perf_counter() - t
-        for m, c, w, f, u, swc, sww in zip(chunk, cold, warm, forced, use, sc_cold, sc_warm):
+        fres = ctx.solve_batch(chunk, options, initial_primal=px, initial_dual=py) if forced else warm
+        t_forced = _t.perf_counter() - t if forced else float("nan")
+        for m, c, w, f, u, swc, sww in zip(chunk, cold, warm, fres, use, sc_cold, sc_warm):
             rows.append(dict(m=m.num_rows, n=m.num_cols, cold_it=c.iterations, warm_it=w.iterations,
                              forced_it=f.iterations, cold_status=c.status.name, warm_status=w.status.name,
                              forced_status=f.status.name, used=int(u), cold_score=swc, warm_score=sww,
@@ -250,6 +250,8 @@ def main() -> None:
     ap.add_argument("--family", default="transport", choices=["transport", "random"],
                     help="transport: S, D in --size; random: the config-0 generator with m in --size, "
                          "n = 3m, 6 nonzeros per column")
+    ap.add_argument("--no-forced", action="store_true",
+                    help="skip the forced (unguarded) warm solves of the evaluation")
     ap.add_argument("--out", default="")
     args = ap.parse_args()
     ctx = Context(0)
@@ -276,7 +278,7 @@ def main() -> None:
     eopt.set_tolerance(args.tol)
     test_models = [family(seed) for seed in range(10_000_000, 10_000_000 + args.test)]
     t0 = time.time()
-    rows = evaluate_batched(ctx, net, test_models, eopt, batch=args.batch)
+    rows = evaluate_batched(ctx, net, test_models, eopt, batch=args.batch, forced=not args.no_forced)
     t_eval = time.time() - t0
     batches = sorted({r["batch"] for r in rows})
     first = {bb: next(r for r in rows if r["batch"] == bb) for bb in batches}
