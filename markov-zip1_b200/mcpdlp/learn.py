@@ -181,6 +181,31 @@ def solve_warm(ctx: Context, net: WarmStartNet, model: Model, options: PdlpOptio
     return ctx.solve(model, o)
 
 
+def train_streaming(ctx: Context, net: WarmStartNet, make, seeds, options: PdlpOptions, batch: int = 256,
+                    passes: int = 3, lr: float = 1e-3, margin: float = 0.05, log=None) -> dict:
+    """Train on many instances without holding them all: for each group of
+    `batch` seeds, build the LPs (`make(seed)`), solve them batched on the
+    GPU for their targets, make `passes` shuffled passes of Adam steps over
+    the group (learning rate halved every pass), then drop the group."""
+    seeds = list(seeds)
+    losses, optimal, t_data, t_train = [], 0, 0.0, 0.0
+    rng = np.random.default_rng(0)
+    for g0 in range(0, len(seeds), batch):
+        t = time.time()
+        data = solve_targets(ctx, [make(sd) for sd in seeds[g0:g0 + batch]], options, batch=batch, margin=margin)
+        t_data += time.time() - t
+        optimal += sum(d.result.status.name == "optimal" for d in data)
+        t = time.time()
+        for p_ in range(passes):
+            for i in rng.permutation(len(data)):
+                losses.append(net.train_step(data[i], lr * (0.5 ** p_)))
+        t_train += time.time() - t
+        if log:
+            log(f"group {g0 // batch}: {len(data)} targets, mean loss {np.mean(losses[-len(data):]):.5f}")
+    return dict(loss_first=float(np.mean(losses[:batch])), loss_last=float(np.mean(losses[-batch:])),
+                target_optimal=optimal, data_s=t_data, train_s=t_train)
+
+
 def start_scores(ctx: Context, models: list, options: PdlpOptions, starts_x=None, starts_y=None) -> list:
     """The reference's KKT score (max of the relative primal and dual
     residuals and the gap, pdlp.cpp:62-135) of each LP's starting point:
@@ -239,7 +264,7 @@ def main() -> None:
     ap.add_argument("--train", type=int, default=20000)
     ap.add_argument("--test", type=int, default=2000)
     ap.add_argument("--batch", type=int, default=256, help="LPs per batched solve")
-    ap.add_argument("--epochs", type=int, default=3)
+    ap.add_argument("--epochs", type=int, default=3, help="passes over each group of targets")
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--target-iterations", type=int, default=20000)
     ap.add_argument("--tol", type=float, default=1e-8)
@@ -263,28 +288,31 @@ def main() -> None:
         S = generators.uniform_int(seed, 0, *args.size)
         D = generators.uniform_int(seed, 1, *args.size)
         return generators.transport(seed, S, D)
-    train_models = [family(seed) for seed in range(args.train)]
     topt = PdlpOptions(max_iterations=args.target_iterations)
     topt.set_tolerance(1e-8)
-    data = solve_targets(ctx, train_models, topt, batch=args.batch, margin=args.margin)
-    t_data = time.time() - t0
     net = WarmStartNet(0, 3, 0)
-    t0 = time.time()
-    hist = net.fit(data, epochs=args.epochs, lr=args.lr, log=print)
-    t_train = time.time() - t0
+    tr = train_streaming(ctx, net, family, range(args.train), topt, batch=args.batch, passes=args.epochs,
+                         lr=args.lr, margin=args.margin, log=print)
     if args.out:
         net.save(args.out)
     eopt = PdlpOptions(max_iterations=args.max_iterations)
     eopt.set_tolerance(args.tol)
-    test_models = [family(seed) for seed in range(10_000_000, 10_000_000 + args.test)]
     t0 = time.time()
-    rows = evaluate_batched(ctx, net, test_models, eopt, batch=args.batch, forced=not args.no_forced)
+    rows = []
+    test_seeds = list(range(10_000_000, 10_000_000 + args.test))
+    for g0 in range(0, len(test_seeds), args.batch):
+        group = [family(sd) for sd in test_seeds[g0:g0 + args.batch]]
+        part = evaluate_batched(ctx, net, group, eopt, batch=args.batch, forced=not args.no_forced)
+        for r in part:
+            r["batch"] = g0 // args.batch
+        rows += part
+        print(f"test group {g0 // args.batch}: cold optimal {sum(r['cold_status'] == 'optimal' for r in part)}, "
+              f"warm optimal {sum(r['warm_status'] == 'optimal' for r in part)}", flush=True)
     t_eval = time.time() - t0
     batches = sorted({r["batch"] for r in rows})
     first = {bb: next(r for r in rows if r["batch"] == bb) for bb in batches}
-    summary = dict(train=args.train, test=args.test, epochs=args.epochs, loss=hist, data_s=t_data,
-                   train_s=t_train, eval_s=t_eval, tol=args.tol, max_iterations=args.max_iterations,
-                   target_optimal=sum(t.result.status.name == "optimal" for t in data),
+    summary = dict(train=args.train, test=args.test, passes=args.epochs, **tr, eval_s=t_eval, tol=args.tol,
+                   max_iterations=args.max_iterations, target_iterations=args.target_iterations,
                    cold_batch_s=float(sum(first[bb]["batch_cold_s"] for bb in batches)),
                    warm_batch_s=float(sum(first[bb]["batch_warm_s"] for bb in batches)),
                    forced_batch_s=float(sum(first[bb]["batch_forced_s"] for bb in batches)),
