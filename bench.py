@@ -520,12 +520,50 @@ def run_engine_arm(args) -> None:
         forms["speedup_time_to_1e-8_fp32_refine_vs_fp64"] = (forms["fp64"]["time_to_tol_s"]
                                                             / forms["fp32_refine"]["time_to_tol_s"])
 
-    # ---- e2e: one full FP64 solve to 1e-8 through the public API from pinned
-    # host buffers; H2D of the model and D2H of the solution in the timed region
+    # ---- the learned warm start (the north star's combined form): a network
+    # trained on GPU-solved LPs of the same generator at small sizes (m in
+    # [200, 600], n = 3m, 1024 seeds), its prediction for this LP fed to the
+    # engine with the guard on (the engine keeps the cold start if the
+    # prediction scores worse); time to 1e-8 includes the prediction
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
     hmodel = mcpdlp.Model(m, n, pin(model.col_start), pin(model.row_index), pin(model.value),
                           pin(model.objective), pin(model.var_lower), pin(model.var_upper),
                           pin(model.row_lower), pin(model.row_upper))
+    if not args.no_learned and not over_budget():
+        from mcpdlp import generators
+        from mcpdlp.learn import WarmStartNet, solve_targets
+        t0 = time.perf_counter()
+        sizes = [generators.uniform_int(sd, 0, 200, 600) for sd in range(1024)]
+        fam = [generators.random_lp(sd, mm, 3 * mm, 6) for sd, mm in enumerate(sizes)]
+        to = PdlpOptions(device=local, max_iterations=20000)
+        to.set_tolerance(1e-8)
+        net = WarmStartNet(local, 3, 0)
+        net.fit(solve_targets(ctx, fam, to, margin=0.0), epochs=6, lr=2e-3)
+        train_s = time.perf_counter() - t0
+        for name, prec in (("fp32_refine_learned_warm", Precision.fp32_refine), ("fp64_learned_warm", Precision.fp64)):
+            if over_budget():
+                forms[name] = {"skipped": f"wall budget of {args.budget_s:.0f} s reached"}
+                continue
+
+            def warm_solve(prec=prec):
+                px, py, _ = net.predict(hmodel)
+                o = options(prec, warm_start_guard=True)
+                o.initial_primal, o.initial_dual = px, py
+                return ctx.solve(hmodel, o)
+            r, el, wall = timed_solve(ctx, torch, stream, dist, dev, warm_solve)
+            forms[name] = {"time_to_tol_s": wall, "iterations": r.iterations, "status": r.status.name,
+                           "objective_rel_err_vs_analytic": abs(r.objective - optimum) / abs(optimum),
+                           "warm_start_used": r.extra["warm_start_used"],
+                           "start_score": {"prediction": r.extra["warm_start_score"],
+                                           "cold": r.extra["cold_start_score"]},
+                           "includes": "prediction (host model), guard, H2D/D2H and the solve",
+                           "training_s": train_s, "training": "1024 GPU-solved LPs of the generator at "
+                                                               "m in [200,600], n = 3m, 6 epochs"}
+            if "time_to_tol_s" in forms.get("fp64", {}):
+                forms[name]["speedup_time_to_1e-8_vs_fp64"] = forms["fp64"]["time_to_tol_s"] / wall
+
+    # ---- e2e: one full FP64 solve to 1e-8 through the public API from pinned
+    # host buffers; H2D of the model and D2H of the solution in the timed region
     h2d_bytes = 4 * (n + 1) + 12 * nnz + 8 * 3 * n + 8 * 2 * m
     d2h_bytes = 8 * (n + m)
     e2e = None
@@ -610,6 +648,7 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start forms")
     ap.add_argument("--budget-s", type=float, default=900.0,
                     help="wall-time budget: legs after it are skipped (the JSON line is still printed)")
     ap.add_argument("--ncu-case", action="store_true",
