@@ -197,22 +197,27 @@ struct EngineBatchMixed : BatchCommon {
     }
 };
 
-// The lanes autotuner: lanes per column for the A^T y kernel and lanes per
-// row for the A x kernel, each chosen by timing that kernel over the batch
-// itself at every power of two 1..32 (best of two timed launches after a
-// warm one).  It runs from the start iterate, which is saved first and put
-// back after, so the solve that follows is the one the chosen lanes give.
-// The choice is kept per context, batch shape and precision: later solves of
-// the same shape reuse it (and repeat bit-identically).
-template <class E>
-int tune_lanes(Ctx& ctx, E& eng, int precision, void* const save_n[3], void* const save_m[2]) {
+// The autotuner: lanes per column for the A^T y kernel and lanes per row for
+// the A x kernel, each chosen by timing that kernel over the batch itself at
+// every power of two 1..32 (best of two timed launches after a warm one);
+// then the block shape of the persistent kernels' work -- lines per tile, 1,
+// 2 or 4 block-steps -- by timing both kernels at each (`retile(steps)`
+// rebuilds the tile tables and the work queue).  Short tiles spread the few
+// LPs that run late in a batch over many blocks; long tiles cut per-tile
+// overhead when the LPs finish together.  It runs from the start iterate,
+// which is saved first and put back after, so the solve that follows is the
+// one the chosen shape gives.  The choice is kept per context, batch shape
+// and precision: later solves of the same shape reuse it (and repeat
+// bit-identically).
+template <class E, class Retile>
+int tune_lanes(Ctx& ctx, E& eng, int precision, void* const save_n[3], void* const save_m[2], Retile&& retile) {
     const auto key = std::make_tuple((long long)eng.P.n, (long long)eng.P.m, (long long)eng.B.nlp,
                                      (long long)eng.B.cols.ntiles * 4 + precision, (long long)eng.B.rows.ntiles);
     auto hit = ctx.lane_cache.find(key);
     if (hit != ctx.lane_cache.end()) {
-        eng.g_col = hit->second.first;
-        eng.g_row = hit->second.second;
-        return MC_OK;
+        eng.g_col = std::get<0>(hit->second);
+        eng.g_row = std::get<1>(hit->second);
+        return retile(std::get<2>(hit->second));
     }
     cudaStream_t s = ctx.stream;
     const size_t elem = sizeof(*eng.P.x);
@@ -225,35 +230,56 @@ int tune_lanes(Ctx& ctx, E& eng, int precision, void* const save_n[3], void* con
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     CU(cudaEventCreate(&e0));
     int rc = ok(cudaEventCreate(&e1), "cudaEventCreate");
+    // best of two timed launches (after a warm one) of primal (which = 0),
+    // dual (1) or both (2) at lanes g
+    auto time_kernels = [&](int which, int g, float* out) -> int {
+        float t_min = 3.0e38f;
+        for (int rep = 0; rep < 3; ++rep) {
+            float ms = 0.f;
+            TRY(ok(cudaEventRecord(e0, s), "cudaEventRecord"));
+            if (which != 1) TRY(eng.primal(ctx, which == 2 ? eng.g_col : g, false, 0));
+            if (which != 0) TRY(eng.dual(ctx, which == 2 ? eng.g_row : g, 0));
+            TRY(ctx.launch_check("autotuner"));
+            TRY(ok(cudaEventRecord(e1, s), "cudaEventRecord"));
+            TRY(ok(cudaEventSynchronize(e1), "cudaEventSynchronize"));
+            TRY(ok(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime"));
+            if (rep > 0 && ms < t_min) t_min = ms;
+        }
+        *out = t_min;
+        return MC_OK;
+    };
     float best[2] = {3.0e38f, 3.0e38f};
     int pick[2] = {eng.g_col, eng.g_row};
     for (int g = 1; g <= 32 && rc == MC_OK; g *= 2) {
         for (int which = 0; which < 2 && rc == MC_OK; ++which) {
-            float t_min = 3.0e38f;
-            for (int rep = 0; rep < 3 && rc == MC_OK; ++rep) {
-                float ms = 0.f;
-                rc = ok(cudaEventRecord(e0, s), "cudaEventRecord");
-                if (rc == MC_OK) rc = which ? eng.dual(ctx, g, 0) : eng.primal(ctx, g, false, 0);
-                if (rc == MC_OK) rc = ctx.launch_check("lanes autotuner");
-                if (rc == MC_OK) rc = ok(cudaEventRecord(e1, s), "cudaEventRecord");
-                if (rc == MC_OK) rc = ok(cudaEventSynchronize(e1), "cudaEventSynchronize");
-                if (rc == MC_OK) rc = ok(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
-                if (rep > 0 && ms < t_min) t_min = ms;
-            }
-            if (rc == MC_OK && t_min < best[which]) {
-                best[which] = t_min;
+            float t = 0.f;
+            rc = time_kernels(which, g, &t);
+            if (rc == MC_OK && t < best[which]) {
+                best[which] = t;
                 pick[which] = g;
             }
         }
     }
+    eng.g_col = pick[0];
+    eng.g_row = pick[1];
+    int steps_pick = 1;
+    float steps_best = 3.0e38f;
+    for (int steps = 1; steps <= 4 && rc == MC_OK; steps *= 2) {
+        float t = 0.f;
+        rc = retile(steps);
+        if (rc == MC_OK) rc = time_kernels(2, 0, &t);
+        if (rc == MC_OK && t < steps_best) {
+            steps_best = t;
+            steps_pick = steps;
+        }
+    }
+    if (rc == MC_OK) rc = retile(steps_pick);
     cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     TRY(rc);
     for (int q = 0; q < 3; ++q) CU(cudaMemcpyAsync(cur_n[q], save_n[q], bn, cudaMemcpyDeviceToDevice, s));
     for (int q = 0; q < 2; ++q) CU(cudaMemcpyAsync(cur_m[q], save_m[q], bm, cudaMemcpyDeviceToDevice, s));
-    eng.g_col = pick[0];
-    eng.g_row = pick[1];
-    ctx.lane_cache[key] = {pick[0], pick[1]};
+    ctx.lane_cache[key] = std::make_tuple(pick[0], pick[1], steps_pick);
     return MC_OK;
 }
 
@@ -468,12 +494,21 @@ int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o,
         host_off[count + b] = lps[b].objective_sense == MC_MAXIMIZE ? -1.0 : 1.0;
     }
     CU(cudaMemcpyAsync(offsets, host_off.data(), sizeof(double) * host_off.size(), cudaMemcpyHostToDevice, s));
+    // tile tables (lp, l0, l1 of every column tile and row tile, then each LP's
+    // tile ranges), in one device buffer sized for the finest tiling
     std::vector<int> tiles_host;
-    tiles_host.reserve(3 * (nct + nrt) + 2 * (count + 1));
-    for (auto* v : {&ct_lp, &ct_l0, &ct_l1, &rt_lp, &rt_l0, &rt_l1, &ct_first, &rt_first})
-        tiles_host.insert(tiles_host.end(), v->begin(), v->end());
     int* tiles = static_cast<int*>(at(o_tiles));
-    CU(cudaMemcpyAsync(tiles, tiles_host.data(), sizeof(int) * tiles_host.size(), cudaMemcpyHostToDevice, s));
+    auto upload_tiles = [&](int steps) -> int {
+        ct_lp.clear(), ct_l0.clear(), ct_l1.clear(), rt_lp.clear(), rt_l0.clear(), rt_l1.clear();
+        make_tiles(col_off, steps * (kBlock / gc), ct_lp, ct_l0, ct_l1, ct_first);
+        make_tiles(row_off, steps * (kBlock / gr), rt_lp, rt_l0, rt_l1, rt_first);
+        tiles_host.clear();
+        for (auto* v : {&ct_lp, &ct_l0, &ct_l1, &rt_lp, &rt_l0, &rt_l1, &ct_first, &rt_first})
+            tiles_host.insert(tiles_host.end(), v->begin(), v->end());
+        CU(cudaMemcpyAsync(tiles, tiles_host.data(), sizeof(int) * tiles_host.size(), cudaMemcpyHostToDevice, s));
+        return MC_OK;
+    };
+    TRY(upload_tiles(1));
     CU(cudaMemsetAsync(ri + nnz, 0, sizeof(int) * 16, s));
     CU(cudaMemsetAsync(cv + nnz, 0, sizeof(double) * 16, s));
     CU(cudaMemsetAsync(ci + nnz, 0, sizeof(int) * 16, s));
@@ -503,17 +538,22 @@ int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o,
     int* active = static_cast<int*>(at(o_active));
     B.active = active;
     B.active_count = active + 2LL * kMaxTiles;
-    int* tp = tiles;
-    B.cols.lp = tp; tp += nct;
-    B.cols.l0 = tp; tp += nct;
-    B.cols.l1 = tp; tp += nct;
-    B.rows.lp = tp; tp += nrt;
-    B.rows.l0 = tp; tp += nrt;
-    B.rows.l1 = tp; tp += nrt;
-    B.cols.first = tp; tp += count + 1;
-    B.rows.first = tp;
-    B.cols.ntiles = nct;
-    B.rows.ntiles = nrt;
+    // point B's tables into the buffer as laid out for the current tiling
+    auto bind_tiles = [&](BatchRefs& R) {
+        const int c = (int)ct_lp.size(), r = (int)rt_lp.size();
+        int* tp = tiles;
+        R.cols.lp = tp; tp += c;
+        R.cols.l0 = tp; tp += c;
+        R.cols.l1 = tp; tp += c;
+        R.rows.lp = tp; tp += r;
+        R.rows.l0 = tp; tp += r;
+        R.rows.l1 = tp; tp += r;
+        R.cols.first = tp; tp += count + 1;
+        R.rows.first = tp;
+        R.cols.ntiles = c;
+        R.rows.ntiles = r;
+    };
+    bind_tiles(B);
 
     // ---- setup: transpose, Ruiz per LP, data per LP
     TRY(build_csr(ctx, (int)m, (int)n, nnz, cs, ri, cv, rs, ci, rv, static_cast<int*>(at(o_cursor)),
@@ -611,9 +651,16 @@ int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o,
         for (int q = 0; q < 3; ++q) save_n[q] = at(o_save_n[q]);
         for (int q = 0; q < 2; ++q) save_m[q] = at(o_save_m[q]);
         const int keep_col = e.g_col, keep_row = e.g_row;
-        TRY(tune_lanes(ctx, e, o->precision, save_n, save_m));
+        // the block shape: tiles of `steps` block-steps, re-bound and re-queued
+        auto retile = [&](int steps) -> int {
+            TRY(upload_tiles(steps));
+            bind_tiles(e.B);
+            return e.compact(ctx);
+        };
+        TRY(tune_lanes(ctx, e, o->precision, save_n, save_m, retile));
         if (valid_lanes(o->lanes_per_column)) e.g_col = keep_col;
         if (valid_lanes(o->lanes_per_row)) e.g_row = keep_row;
+        B = e.B;  // the tables the solve ran with (for the output stage)
         return MC_OK;
     };
     float* f_xa = nullptr;
@@ -708,7 +755,7 @@ int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o,
 
     // ---- outputs
     ctx.begin_launch(MC_KERNEL_OTHER);
-    kb_unscale_out<<<nct + nrt, kBlock, 0, s>>>(mixed ? P.x : P.x_avg, f_xa, mixed ? P.y : P.y_avg, f_ya, col_scale,
+    kb_unscale_out<<<B.cols.ntiles + B.rows.ntiles, kBlock, 0, s>>>(mixed ? P.x : P.x_avg, f_xa, mixed ? P.y : P.y_avg, f_ya, col_scale,
                                                 row_scale, stage_x, stage_y, B);
     ctx.end_launch();
     TRY(ctx.launch_check("batch unscale"));

@@ -78,8 +78,10 @@ struct Ctx {
     cudaEvent_t ev_a = nullptr, ev_b = nullptr, ev_c = nullptr, ev_d = nullptr;
     cudaEvent_t ev_poll[2] = {nullptr, nullptr};
     std::map<int, cudaGraphExec_t> graphs;
-    // batch lanes chosen by the autotuner, per batch shape (n, m, LPs, tiles)
-    std::map<std::tuple<long long, long long, long long, long long, long long>, std::pair<int, int>> lane_cache;
+    // batch lanes and tile size chosen by the autotuner, per batch shape (n, m, LPs, tiles):
+    // lanes per column, lanes per row, block-steps per tile
+    std::map<std::tuple<long long, long long, long long, long long, long long>, std::tuple<int, int, int>>
+        lane_cache;
 
     // launch accounting / profiling
     bool profiling = false;
