@@ -540,7 +540,7 @@ def run_engine_arm(args) -> None:
         net = WarmStartNet(local, 3, 0)
         net.fit(solve_targets(ctx, fam, to, margin=0.0), epochs=6, lr=2e-3)
         train_s = time.perf_counter() - t0
-        for name, prec in (("fp32_refine_learned_warm", Precision.fp32_refine), ("fp64_learned_warm", Precision.fp64)):
+        for name, prec in (("fp32_refine_learned_warm", Precision.fp32_refine),):
             if over_budget():
                 forms[name] = {"skipped": f"wall budget of {args.budget_s:.0f} s reached"}
                 continue

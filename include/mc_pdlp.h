@@ -109,9 +109,7 @@ typedef struct mc_pdlp_options {
     int32_t lanes_per_column;         /* A^T y kernel: 0 = automatic (single LP: by mean
                                          column length; batch: the lanes autotuner, timed on
                                          the batch and kept per context and batch shape),
-                                         -1 = one thread per column over shared-memory
-                                         tiles (single LP only), 1..32 (power of two) =
-                                         lanes per column */
+                                         1..32 (power of two) = lanes per column */
     int32_t lanes_per_row;            /* A x kernel, same meaning per row */
     int32_t warm_start_guard;         /* 1: with a warm start, evaluate the reference's KKT score
                                          of the warm start and of the cold start (x = proj(0),

@@ -313,8 +313,6 @@ int solve_batch(Ctx& ctx, const mc_lp* lps, int count, const mc_pdlp_options* o,
     if (!lps || count <= 0 || !results) return set_error(MC_ERR_INVALID_ARGUMENT, "empty batch");
     TRY(validate_options(o));
     const bool mixed = o->precision == MC_PRECISION_FP32_REFINE;
-    if (o->lanes_per_column == -1 || o->lanes_per_row == -1)
-        return set_error(MC_ERR_INVALID_ARGUMENT, "batched solves use the lane kernels");
     std::vector<long long> col_off(count + 1, 0), row_off(count + 1, 0), nnz_off(count + 1, 0);
     for (int b = 0; b < count; ++b) {
         std::memset(&results[b], 0, sizeof(mc_pdlp_result));

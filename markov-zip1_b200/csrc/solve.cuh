@@ -4,7 +4,6 @@
 #include "engine.hpp"
 #include "iter_kernels.cuh"
 #include "setup_kernels.cuh"
-#include "staged.cuh"
 #include "mixed.cuh"
 
 #include <climits>
@@ -24,20 +23,22 @@ namespace mc {
         default: { constexpr int G = 32; __VA_ARGS__; } break; \
     }
 
-// Launch geometry of one problem: per side either the tile-staged kernels
-// (one thread per line, matrix through shared memory) or the lane kernels
-// (G lanes per line, for long lines), and grid sizes (one wave of resident
-// blocks per kernel; the reduction partial counts follow the grids, so they
-// are fixed per plan).
+// Launch geometry of one problem: G lanes per line for each side, and grid
+// sizes (one wave of resident blocks per kernel; the reduction partial counts
+// follow the grids, so they are fixed per plan).
+//
+// (Tile-staged kernels -- one thread per line, the matrix slice of an
+// nnz-balanced tile copied into shared memory with double-buffered cp.async --
+// were built and measured on B200 at the 40M-nonzero LP: 0.406 / 0.307 ms
+// per primal / dual launch against 0.244 / 0.245 for the lane kernels, so
+// they were dropped.)
 struct Plan {
-    bool staged_col = false, staged_row = false;
     int g_col = 1, g_row = 1;
     int g_probe = 1;                      // lanes per row of the step-size probe
     int nb_col = 1, nb_row = 1;           // primal / dual SpMV kernels
     int nb_col_step = 1, nb_row_step = 1; // step-size variants (they write partials)
     int nb_res_col = 1, nb_res_row = 1;   // residual kernels
     int nb_m = 1, nb_nm = 1;              // elementwise kernels over m / n+m
-    Tiles tiles{};
 };
 
 static int valid_lanes(int g) { return g == 1 || g == 2 || g == 4 || g == 8 || g == 16 || g == 32; }
@@ -47,61 +48,26 @@ static int valid_lanes(int g) { return g == 1 || g == 2 || g == 4 || g == 8 || g
 // (measured on B200 at 20 entries per row: 0.52 ms at 8 lanes vs 0.62 ms at 4).
 static int probe_lanes(int g_row) { return g_row < 32 ? 2 * g_row : 32; }
 
-// lanes option: 0 = lanes chosen by mean line length, -1 = staged, 1..32 = lanes
-
+// lanes option: 0 = lanes chosen by mean line length, 1..32 = lanes
 template <class T>
-Plan make_plan(const Ctx& ctx, int m, int n, long long nnz, int force_col, int force_row,
-               const int* col_bounds, const int* row_bounds) {
+Plan make_plan(const Ctx& ctx, int m, int n, long long nnz, int force_col, int force_row) {
     Plan p;
     const double mean_col = n > 0 ? (double)nnz / n : 1.0;
     const double mean_row = m > 0 ? (double)nnz / m : 1.0;
-    p.staged_col = force_col == -1;
-    p.staged_row = force_row == -1;
     p.g_col = valid_lanes(force_col) ? force_col : pick_lanes(mean_col);
     p.g_row = valid_lanes(force_row) ? force_row : pick_lanes(mean_row);
     p.g_probe = probe_lanes(p.g_row);
-    const int chunk = stage_chunk<T>();
-    p.tiles.col_bounds = col_bounds;
-    p.tiles.row_bounds = row_bounds;
-    p.tiles.ncol_tiles = (int)std::max<long long>(1, (nnz + chunk - 1) / chunk);
-    p.tiles.nrow_tiles = p.tiles.ncol_tiles;
-    const size_t sm = staged_smem_bytes<T>();
-    if (p.staged_col) {
-        p.nb_col = grid_for(ctx, k_primal_staged<false, T>, p.tiles.ncol_tiles, 1, sm);
-        p.nb_col_step = grid_for(ctx, k_primal_staged<true, T>, p.tiles.ncol_tiles, 1, sm);
-    } else {
-        MC_DISPATCH_G(p.g_col, {
-            p.nb_col = grid_for(ctx, k_primal<G, false, T>, n, kBlock / G);
-            p.nb_col_step = grid_for(ctx, k_primal<G, true, T>, n, kBlock / G);
-        });
-    }
-    if (p.staged_row) {
-        p.nb_row = grid_for(ctx, k_dual_staged<T>, p.tiles.nrow_tiles, 1, sm);
-        p.nb_row_step = grid_for(ctx, k_dual_probe_staged<T>, p.tiles.nrow_tiles, 1, sm);
-    } else {
-        MC_DISPATCH_G(p.g_row, p.nb_row = grid_for(ctx, k_dual<G, T>, m, kBlock / G));
-        MC_DISPATCH_G(p.g_probe, p.nb_row_step = grid_for(ctx, k_dual_probe<G, T>, m, kBlock / G));
-    }
+    MC_DISPATCH_G(p.g_col, {
+        p.nb_col = grid_for(ctx, k_primal<G, false, T>, n, kBlock / G);
+        p.nb_col_step = grid_for(ctx, k_primal<G, true, T>, n, kBlock / G);
+    });
+    MC_DISPATCH_G(p.g_row, p.nb_row = grid_for(ctx, k_dual<G, T>, m, kBlock / G));
+    MC_DISPATCH_G(p.g_probe, p.nb_row_step = grid_for(ctx, k_dual_probe<G, T>, m, kBlock / G));
     MC_DISPATCH_G(p.g_col, p.nb_res_col = grid_for(ctx, k_residual_cols<G, T>, n, kBlock / G));
     MC_DISPATCH_G(p.g_row, p.nb_res_row = grid_for(ctx, k_residual_rows<G, T>, m, kBlock / G));
     p.nb_m = grid_for(ctx, k_dual_apply<T>, m, kBlock);
     p.nb_nm = grid_for(ctx, k_restart_copy<T>, (long long)n + m, kBlock);
     return p;
-}
-
-// tile boundaries of both copies (once per solve)
-int build_tiles(Ctx& ctx, const Plan& p, int m, int n, const int* csc_start, const int* csr_start,
-                int* col_bounds, int* row_bounds, int chunk) {
-    cudaStream_t s = ctx.stream;
-    ctx.begin_launch(MC_KERNEL_SETUP);
-    k_tile_bounds<<<(p.tiles.ncol_tiles + kBlock) / kBlock, kBlock, 0, s>>>(n, csc_start, chunk, p.tiles.ncol_tiles,
-                                                                            col_bounds);
-    ctx.end_launch();
-    ctx.begin_launch(MC_KERNEL_SETUP);
-    k_tile_bounds<<<(p.tiles.nrow_tiles + kBlock) / kBlock, kBlock, 0, s>>>(m, csr_start, chunk, p.tiles.nrow_tiles,
-                                                                            row_bounds);
-    ctx.end_launch();
-    return ctx.launch_check("tile bounds");
 }
 
 // ------------------------------------------------------------- transpose
@@ -234,12 +200,8 @@ struct Engine64 {
 
     int iteration(Ctx& ctx, int k, bool step, const Controls& ctl) const {
         cudaStream_t s = ctx.stream;
-        const size_t sm = staged_smem_bytes<double>();
         ctx.begin_launch(MC_KERNEL_PRIMAL);
-        if (pl.staged_col) {
-            if (step) k_primal_staged<true, double><<<pl.nb_col_step, kBlock, sm, s>>>(P, pl.tiles, k);
-            else k_primal_staged<false, double><<<pl.nb_col, kBlock, sm, s>>>(P, pl.tiles, k);
-        } else if (step) {
+        if (step) {
             MC_DISPATCH_G(pl.g_col, (k_primal<G, true, double><<<pl.nb_col_step, kBlock, 0, s>>>(P, k)));
         } else {
             MC_DISPATCH_G(pl.g_col, (k_primal<G, false, double><<<pl.nb_col, kBlock, 0, s>>>(P, k)));
@@ -247,11 +209,7 @@ struct Engine64 {
         ctx.end_launch();
         if (step) {
             ctx.begin_launch(MC_KERNEL_DUAL_STEP);
-            if (pl.staged_row) {
-                k_dual_probe_staged<double><<<pl.nb_row_step, kBlock, sm, s>>>(P, pl.tiles);
-            } else {
-                MC_DISPATCH_G(pl.g_probe, (k_dual_probe<G, double><<<pl.nb_row_step, kBlock, 0, s>>>(P)));
-            }
+            MC_DISPATCH_G(pl.g_probe, (k_dual_probe<G, double><<<pl.nb_row_step, kBlock, 0, s>>>(P)));
             ctx.end_launch();
             ctx.begin_launch(MC_KERNEL_OTHER);
             k_step_size<<<1, 1024, 0, s>>>(P.partials, pl.nb_col_step, pl.nb_row_step, P.st, ctl);
@@ -261,11 +219,7 @@ struct Engine64 {
             ctx.end_launch();
         } else {
             ctx.begin_launch(MC_KERNEL_DUAL);
-            if (pl.staged_row) {
-                k_dual_staged<double><<<pl.nb_row, kBlock, sm, s>>>(P, pl.tiles, k);
-            } else {
-                MC_DISPATCH_G(pl.g_row, (k_dual<G, double><<<pl.nb_row, kBlock, 0, s>>>(P, k)));
-            }
+            MC_DISPATCH_G(pl.g_row, (k_dual<G, double><<<pl.nb_row, kBlock, 0, s>>>(P, k)));
             ctx.end_launch();
         }
         return ctx.launch_check("iteration");
@@ -547,11 +501,9 @@ int validate_options(const mc_pdlp_options* o) {
         return set_error(MC_ERR_INVALID_ARGUMENT, "unknown restart_strategy %d", o->restart_strategy);
     if (o->precision != MC_PRECISION_FP64 && o->precision != MC_PRECISION_FP32_REFINE)
         return set_error(MC_ERR_INVALID_ARGUMENT, "unknown precision %d", o->precision);
-    if ((o->lanes_per_column && o->lanes_per_column != -1 && !valid_lanes(o->lanes_per_column)) ||
-        (o->lanes_per_row && o->lanes_per_row != -1 && !valid_lanes(o->lanes_per_row)))
-        return set_error(MC_ERR_INVALID_ARGUMENT, "lanes per line must be 0, -1 or a power of two <= 32");
-    if (o->precision == MC_PRECISION_FP32_REFINE && (o->lanes_per_column == -1 || o->lanes_per_row == -1))
-        return set_error(MC_ERR_INVALID_ARGUMENT, "the staged kernels are FP64 only");
+    if ((o->lanes_per_column && !valid_lanes(o->lanes_per_column)) ||
+        (o->lanes_per_row && !valid_lanes(o->lanes_per_row)))
+        return set_error(MC_ERR_INVALID_ARGUMENT, "lanes per line must be 0 or a power of two <= 32");
     return MC_OK;
 }
 
@@ -655,10 +607,6 @@ int begin_session(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const dou
     const size_t o_csr_start = L.add<int>(m + 1);
     const size_t o_csr_col = L.add<int>(nnz + 16);
     const size_t o_csr_val = L.add<double>(nnz + 16);
-    const int chunk = stage_chunk<double>();
-    const long long ntiles = std::max<long long>(1, (nnz + chunk - 1) / chunk);
-    const size_t o_col_bounds = L.add<int>(ntiles + 1);
-    const size_t o_row_bounds = L.add<int>(ntiles + 1);
     const size_t o_cursor = L.add<int>(m);
     const size_t o_long = L.add<int>(m);
     const size_t o_counters = L.add<int>(4);
@@ -844,10 +792,7 @@ int begin_session(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const dou
         P.partials = partials;
         P.st = st;
         eng.O = O;
-        eng.pl = make_plan<double>(ctx, m, n, nnz, o->lanes_per_column, o->lanes_per_row,
-                                   static_cast<int*>(at(o_col_bounds)), static_cast<int*>(at(o_row_bounds)));
-        TRY(build_tiles(ctx, eng.pl, m, n, csc_start, csr_start, static_cast<int*>(at(o_col_bounds)),
-                        static_cast<int*>(at(o_row_bounds)), chunk));
+        eng.pl = make_plan<double>(ctx, m, n, nnz, o->lanes_per_column, o->lanes_per_row);
         TRY(choose_start(ctx, eng, st, ctl, have_warm, o->warm_start_guard != 0, start, [] { return MC_OK; }, res));
     } else {
         EngineMixed& eng = SS.emx;
@@ -929,8 +874,7 @@ int begin_session(Ctx& ctx, const mc_lp* lp, const mc_pdlp_options* o, const dou
         M.r_hi = f_rhi;
         M.yb = f_yb;
         eng.O = O;
-        eng.pl = make_plan<float>(ctx, m, n, nnz, o->lanes_per_column, o->lanes_per_row,
-                                  static_cast<int*>(at(o_col_bounds)), static_cast<int*>(at(o_row_bounds)));
+        eng.pl = make_plan<float>(ctx, m, n, nnz, o->lanes_per_column, o->lanes_per_row);
         // the FP32 dual kernel has no block partials: one block per kBlock/G rows
         // (about 40 waves) lets the block scheduler even out the last wave,
         // 13% faster on B200 than one resident wave; the FP64 and primal

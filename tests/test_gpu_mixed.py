@@ -89,6 +89,8 @@ def test_iteration_limit_edges(gpu_ctx, max_iterations):
     assert res.iterations == max_iterations
 
 
-def test_staged_kernels_rejected_in_mixed_form(gpu_ctx):
-    with pytest.raises(ValueError, match="FP64 only"):
+def test_invalid_lanes_rejected(gpu_ctx):
+    with pytest.raises(ValueError, match="power of two"):
         gpu_ctx.solve(synthetic("small_s7"), mixed(1e-6, lanes_per_row=-1))
+    with pytest.raises(ValueError, match="power of two"):
+        gpu_ctx.solve(synthetic("small_s7"), mixed(1e-6, lanes_per_column=3))
