@@ -322,13 +322,16 @@ def run_batch_ncu_case(args) -> None:
     """A short batched solve of the batch workload (for ncu captures)."""
     import mcpdlp
     from mcpdlp import PdlpOptions, Precision
-    models, _, _ = batch_models(args.workload)
+    models, _, base = batch_models(args.workload)
     ctx = mcpdlp.Context(0)
     o = PdlpOptions(max_iterations=args.ncu_iterations, profile_kernels=True,
                     precision=Precision.fp32_refine if args.precision == "fp32_refine" else Precision.fp64)
     o.set_tolerance(1e-6)
-    res = ctx.solve_batch(models, o)
-    print(json.dumps({"ncu_case": args.workload, "precision": args.precision,
+    if args.shared_matrix and base is not None:
+        res = ctx.solve_variants(base, [m_.var_lower for m_ in models], [m_.var_upper for m_ in models], o)
+    else:
+        res = ctx.solve_batch(models, o)
+    print(json.dumps({"ncu_case": args.workload, "precision": args.precision, "shared_matrix": args.shared_matrix,
                       "iterations": max(r.iterations for r in res),
                       "launches": res[0].extra["launches_by_kind"]}), flush=True)
     ctx.close()
@@ -654,6 +657,8 @@ def main() -> None:
     ap.add_argument("--ncu-case", action="store_true",
                     help="run one short profiled solve of the workload (for ncu) and exit")
     ap.add_argument("--ncu-iterations", type=int, default=12)
+    ap.add_argument("--shared-matrix", action="store_true",
+                    help="with --ncu-case --workload batch2: the variant solve (one matrix) instead of the packed batch")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32_refine"])
     ap.add_argument("--workload", default="config1", choices=["config1", "config2", "batch1", "batch2"])
     args = ap.parse_args()
