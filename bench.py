@@ -333,7 +333,8 @@ def run_batch_ncu_case(args) -> None:
         res = ctx.solve_batch(models, o)
     print(json.dumps({"ncu_case": args.workload, "precision": args.precision, "shared_matrix": args.shared_matrix,
                       "iterations": max(r.iterations for r in res),
-                      "launches": res[0].extra["launches_by_kind"]}), flush=True)
+                      "launches": res[0].extra["launches_by_kind"],
+                      "kernel_ms": res[0].extra["kernel_ms_by_kind"]}), flush=True)
     ctx.close()
 
 
