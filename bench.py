@@ -372,14 +372,14 @@ def run_batch_arm(args) -> None:
     el, res = timed(Precision.fp32_refine)
     el64, res64 = timed(Precision.fp64)
     lps = sum_over_ranks(dist, float(len(models) * args.steps), dev)
-    shared = None
+    shared = {}
     if base is not None:
         # the node variants with the matrix read once per iteration for all of them
-        ov = PdlpOptions(device=local)
-        ov.set_tolerance(1e-6)
         lows, ups = [m_.var_lower for m_ in models], [m_.var_upper for m_ in models]
-        elv, resv = timed(Precision.fp64, lambda: ctx.solve_variants(base, lows, ups, ov))
-        shared = (elv, resv)
+        for form, prec in (("fp64", Precision.fp64), ("fp32_refine", Precision.fp32_refine)):
+            ov = PdlpOptions(device=local, precision=prec)
+            ov.set_tolerance(1e-6)
+            shared[form] = timed(prec, lambda ov=ov: ctx.solve_variants(base, lows, ups, ov))
 
     def summary(rs):
         st = [r.status.name for r in rs]
@@ -402,12 +402,12 @@ def run_batch_arm(args) -> None:
                       "fp64": {"LPs_per_s": lps / el64, "ms_per_step": el64 * 1e3 / args.steps,
                                **summary(res64)}},
             "gpu_launches": res[0].extra["kernel_launches"] * args.steps}
-    if shared is not None:
-        elv, resv = shared
-        agree = sum(1 for a, b in zip(resv, res64) if a.status == b.status)
-        line["forms"]["shared_matrix_fp64"] = {
+    for form, (elv, resv) in shared.items():
+        packed_el, packed_res = (el64, res64) if form == "fp64" else (el, res)
+        agree = sum(1 for a, b in zip(resv, packed_res) if a.status == b.status)
+        line["forms"][f"shared_matrix_{form}"] = {
             "LPs_per_s": lps / elv, "ms_per_step": elv * 1e3 / args.steps,
-            "speedup_vs_packed_fp64": el64 / elv, "status_agrees_with_packed": f"{agree}/{len(models)}",
+            "speedup_vs_packed_same_form": packed_el / elv, "status_agrees_with_packed": f"{agree}/{len(models)}",
             "engine": "mc_pdlp_ctx_solve_variants: one matrix, variant-minor iterates", **summary(resv)}
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -332,7 +332,9 @@ int mc_pdlp_ctx_solve_batch_warm(mc_pdlp_ctx* ctx, const mc_lp* lps, int32_t cou
  * termination); results[b], primal_out[b] / dual_out[b] (may be NULL) as for
  * the batch.  Infeasible variants end with INFEASIBLE_OR_UNBOUNDED and a
  * certificate (crossed bounds, row activity, or a dual ray in dual_out[b]).
- * FP64 form only.
+ * Both precision forms: MC_PRECISION_FP32_REFINE runs each variant as an
+ * FP64 base plus an FP32 correction, re-centred at every restart, as the
+ * single-LP form does.
  */
 int mc_pdlp_ctx_solve_variants(mc_pdlp_ctx* ctx, const mc_lp* base, int32_t count,
                                const double* const* var_lower, const double* const* var_upper,

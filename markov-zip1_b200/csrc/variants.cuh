@@ -639,6 +639,387 @@ struct EngineVariants {
     }
 };
 
+// ----------------------------------------------------- the FP32 form
+// The mixed-precision form of mixed.cuh per variant: each variant's iterate
+// is an FP64 base plus an FP32 correction, x = xh + dx, y = yh + dy; FP32 PDHG
+// runs on the correction LP (FP32 matrix, FP32 variant-minor vectors); the
+// residual pass, gap, restart test and primal weight are FP64 on xh + dx_avg
+// with the FP64 matrix; at every restart a variant's base moves to its average
+// and its correction LP is rebuilt from the residual pass's FP64 products.
+struct VarMixed {
+    const int* cs;          // the base's CSC / CSR structure (shared with the FP64 data)
+    const int* ri;
+    const float* cv;        // FP32 matrix values
+    const int* rs;
+    const int* ci;
+    const float* rv;
+    const float* col_norm;  // FP32 norms
+    const float* row_norm;
+    const double* c64;      // scaled c, FP64
+    const double* blo64;    // scaled row bounds, sentinel form, FP64
+    const double* bhi64;
+    double* xh;             // [n Kp] FP64 bases
+    double* yh;             // [m Kp]
+    double* axf;            // [m Kp] A (xh + dx_avg) from the residual pass
+    double* atyf;           // [n Kp] A^T (yh + dy_avg)
+    float* x;               // [n Kp] dx
+    float* xb;              // [n Kp] dx-bar
+    float* xa;              // [n Kp] dx average
+    float* xdx;             // [2 n Kp] (dx-bar, d dx) pairs
+    float* g;               // [n Kp] float(c + A^T yh)
+    float* lo;              // [n Kp] float(lo - xh), +-inf when unbounded
+    float* hi;
+    float* y;               // [m Kp] dy
+    float* ya;              // [m Kp] dy average
+    float* axb;             // [m Kp] A dx-bar of a step-size iteration
+    float* yb;              // [m Kp] float(yh)
+    float* rlo;             // [m Kp] float(A xh - b_lo), +inf when unbounded
+    float* rhi;             // [m Kp] float(A xh - b_hi), -inf when unbounded
+};
+
+__device__ __forceinline__ float variant_dot_f(const int* __restrict__ start, const int* __restrict__ idx,
+                                               const float* __restrict__ val, const float* __restrict__ v, int Kp,
+                                               long long l, int k, bool live, unsigned long long pol) {
+    const int b = __ldg(start + l), e = __ldg(start + l + 1);
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+    int p = b;
+    for (; p + 4 <= e; p += 4) {
+        const int i0 = __ldg(idx + p), i1 = __ldg(idx + p + 1), i2 = __ldg(idx + p + 2), i3 = __ldg(idx + p + 3);
+        const float a0 = __ldg(val + p), a1 = __ldg(val + p + 1), a2 = __ldg(val + p + 2), a3 = __ldg(val + p + 3);
+        if (live) {
+            s0 = fmaf(a0, ld_keep(v + (size_t)i0 * Kp + k, pol), s0);
+            s1 = fmaf(a1, ld_keep(v + (size_t)i1 * Kp + k, pol), s1);
+            s2 = fmaf(a2, ld_keep(v + (size_t)i2 * Kp + k, pol), s2);
+            s3 = fmaf(a3, ld_keep(v + (size_t)i3 * Kp + k, pol), s3);
+        }
+    }
+    for (; p < e; ++p)
+        if (live) s0 = fmaf(__ldg(val + p), ld_keep(v + (size_t)__ldg(idx + p) * Kp + k, pol), s0);
+    return (s0 + s1) + (s2 + s3);
+}
+
+template <bool STEP>
+__global__ void __launch_bounds__(kBlock) kvm_primal(int n, VarRefs V, VarMixed M, int kk) {
+    __shared__ double sm[kVarWarps][33];
+    MC_VARIANT_LANE(V, k, live);
+    float step = 0.f, cnt = 1.f;
+    if (live) {
+        const DevState& s = V.st[k];
+        step = (float)(s.eta / s.omega);
+        cnt = (float)(double)(s.avg_count + kk + 1);
+    }
+    const unsigned long long pol = policy_keep();
+    double acc = 0.0;
+    MC_VARIANT_LINES(j, n) {
+        const float aty = variant_dot_f(M.cs, M.ri, M.cv, M.y, V.Kp, j, k, live, pol);
+        if (live) {
+            const size_t q = (size_t)j * V.Kp + k;
+            const float cn = __ldg(M.col_norm + j);
+            const float g = __fadd_rn(ld_stream(M.g + q), aty);
+            const float tau = __fdiv_rn(step, cn);
+            const float xo = ld_stream(M.x + q);
+            const float xp = clampv(__fsub_rn(xo, __fmul_rn(tau, g)), ld_stream(M.lo + q), ld_stream(M.hi + q));
+            const float d = __fsub_rn(xp, xo);
+            const float xbar = __fsub_rn(__fmul_rn(2.f, xp), xo);
+            if (STEP) {
+                st_keep2(M.xdx + 2 * q, xbar, d, pol);
+                acc += __dmul_rn(__dmul_rn((double)cn, (double)d), (double)d);
+            } else {
+                st_keep(M.xb + q, xbar, pol);
+            }
+            st_stream(M.x + q, xp);
+            const float xa = ld_stream(M.xa + q);
+            st_stream(M.xa + q, __fadd_rn(xa, __fdiv_rn(__fsub_rn(xp, xa), cnt)));
+        }
+    }
+    if (STEP) {
+        acc = lanes_reduce(acc, sm, OpSum());
+        if ((threadIdx.x >> 5) == 0 && k < V.K) var_partial(V, SLOT_DX, k)[blockIdx.x] = acc;
+    }
+}
+
+// the dual step on the correction (dual_update_mx of mixed.cuh, per variant)
+__device__ __forceinline__ void variant_dual_update_mx(const VarRefs& V, const VarMixed& M, long long i, int k,
+                                                       float ax, float sg, float cnt, unsigned long long pol) {
+    const size_t q = (size_t)i * V.Kp + k;
+    const float sigma = __fdiv_rn(sg, __ldg(M.row_norm + i));
+    const float dy = ld_stream(M.y + q), yb = ld_stream(M.yb + q);
+    const float rl = ld_stream(M.rlo + q), rh = ld_stream(M.rhi + q);
+    const float base = __fdiv_rn(__fadd_rn(yb, dy), sigma);
+    float dyn;
+    if (__fadd_rn(base, __fadd_rn(rl, ax)) < 0.f) dyn = __fadd_rn(dy, __fmul_rn(sigma, __fadd_rn(rl, ax)));
+    else if (__fadd_rn(base, __fadd_rn(rh, ax)) > 0.f) dyn = __fadd_rn(dy, __fmul_rn(sigma, __fadd_rn(rh, ax)));
+    else dyn = -yb;
+    st_keep(M.y + q, dyn, pol);
+    const float dya = ld_stream(M.ya + q);
+    st_stream(M.ya + q, __fadd_rn(dya, __fdiv_rn(__fsub_rn(dyn, dya), cnt)));
+}
+
+__global__ void __launch_bounds__(kBlock) kvm_dual(int m, VarRefs V, VarMixed M, int kk) {
+    MC_VARIANT_LANE(V, k, live);
+    float sg = 0.f, cnt = 1.f;
+    if (live) {
+        const DevState& s = V.st[k];
+        sg = (float)(s.eta * s.omega);
+        cnt = (float)(double)(s.avg_count + kk + 1);
+    }
+    const unsigned long long pol = policy_keep();
+    MC_VARIANT_LINES(i, m) {
+        const float ax = variant_dot_f(M.rs, M.ci, M.rv, M.xb, V.Kp, i, k, live, pol);
+        if (live) variant_dual_update_mx(V, M, i, k, ax, sg, cnt, pol);
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) kvm_dual_probe(int m, VarRefs V, VarMixed M) {
+    __shared__ double sm[kVarWarps][33];
+    MC_VARIANT_LANE(V, k, live);
+    const unsigned long long pol = policy_keep();
+    double acc = 0.0;
+    MC_VARIANT_LINES(i, m) {
+        const int b = __ldg(M.rs + i), e = __ldg(M.rs + i + 1);
+        float sv0 = 0.f, sw0 = 0.f, sv1 = 0.f, sw1 = 0.f;
+        int p = b;
+        for (; p + 2 <= e; p += 2) {
+            const int j0 = __ldg(M.ci + p), j1 = __ldg(M.ci + p + 1);
+            const float a0 = __ldg(M.rv + p), a1 = __ldg(M.rv + p + 1);
+            if (live) {
+                float v0, w0, v1, w1;
+                ld_keep2(M.xdx + 2 * ((size_t)j0 * V.Kp + k), pol, v0, w0);
+                ld_keep2(M.xdx + 2 * ((size_t)j1 * V.Kp + k), pol, v1, w1);
+                sv0 = fmaf(a0, v0, sv0);
+                sw0 = fmaf(a0, w0, sw0);
+                sv1 = fmaf(a1, v1, sv1);
+                sw1 = fmaf(a1, w1, sw1);
+            }
+        }
+        if (p < e && live) {
+            float v0, w0;
+            ld_keep2(M.xdx + 2 * ((size_t)__ldg(M.ci + p) * V.Kp + k), pol, v0, w0);
+            const float a0 = __ldg(M.rv + p);
+            sv0 = fmaf(a0, v0, sv0);
+            sw0 = fmaf(a0, w0, sw0);
+        }
+        if (live) {
+            M.axb[(size_t)i * V.Kp + k] = sv0 + sv1;
+            const double adx = (double)(sw0 + sw1);
+            acc += __ddiv_rn(__dmul_rn(adx, adx), (double)__ldg(M.row_norm + i));
+        }
+    }
+    acc = lanes_reduce(acc, sm, OpSum());
+    if ((threadIdx.x >> 5) == 0 && k < V.K) var_partial(V, SLOT_ADX, k)[blockIdx.x] = acc;
+}
+
+__global__ void __launch_bounds__(kBlock) kvm_dual_apply(int m, VarRefs V, VarMixed M, int kk) {
+    MC_VARIANT_LANE(V, k, live);
+    if (!live) return;  // no barrier follows
+    const DevState& s = V.st[k];
+    const float sg = (float)(s.eta * s.omega);
+    const float cnt = (float)(double)(s.avg_count + kk + 1);
+    const unsigned long long pol = policy_keep();
+    MC_VARIANT_LINES(i, m) variant_dual_update_mx(V, M, i, k, M.axb[(size_t)i * V.Kp + k], sg, cnt, pol);
+}
+
+// FP64 residual pass on xh + dx_avg, yh + dy_avg (FP64 matrix of the base),
+// keeping A x and A^T y of that point for the recentring; Farkas terms.
+__global__ void __launch_bounds__(kBlock) kvm_residual_rows(VarBase Bs, VarRefs V, VarMixed M, Original O) {
+    __shared__ double sm[kVarWarps][33];
+    MC_VARIANT_LANE(V, k, live);
+    RowTerms acc;
+    RayTerms ray;
+    MC_VARIANT_LINES(i, Bs.m) {
+        double s = 0.0;
+        if (live) {
+            for (int p = __ldg(Bs.rs + i); p < __ldg(Bs.rs + i + 1); ++p) {
+                const size_t qj = (size_t)__ldg(Bs.ci + p) * V.Kp + k;
+                s = fma(__ldg(Bs.rv + p), M.xh[qj] + (double)M.xa[qj], s);
+            }
+            const size_t q = (size_t)i * V.Kp + k;
+            M.axf[q] = s;
+            const double yv = M.yh[q] + (double)M.ya[q];
+            acc.add(O, (int)i, s, yv);
+            const double d = RayTerms::candidate(O, (int)i, yv, V.y_prev + q);
+            V.dray[q] = d;
+            ray.add_row(O, (int)i, d);
+        }
+    }
+    const double vmax = lanes_reduce(acc.vmax, sm, OpMax());
+    const double dsum = lanes_reduce(acc.dsum, sm, OpSum());
+    const double bad = lanes_reduce(acc.bad, sm, OpSum());
+    const double ru = lanes_reduce(ray.u, sm, OpSum());
+    const double rsc = lanes_reduce(ray.rscale, sm, OpSum());
+    const double rinf = lanes_reduce(ray.rinf, sm, OpSum());
+    if ((threadIdx.x >> 5) == 0 && k < V.K) {
+        var_partial(V, SLOT_ROW_MAX, k)[blockIdx.x] = vmax;
+        var_partial(V, SLOT_ROW_DOBJ, k)[blockIdx.x] = dsum;
+        var_partial(V, SLOT_NAN, k)[blockIdx.x] = bad;
+        var_partial(V, SLOT_RAY_U, k)[blockIdx.x] = ru;
+        var_partial(V, SLOT_RAY_RSCALE, k)[blockIdx.x] = rsc;
+        var_partial(V, SLOT_RAY_RINF, k)[blockIdx.x] = rinf;
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) kvm_residual_cols(VarBase Bs, VarRefs V, VarMixed M, Original O) {
+    __shared__ double sm[kVarWarps][33];
+    MC_VARIANT_LANE(V, k, live);
+    ColTerms acc;
+    RayTerms ray;
+    MC_VARIANT_LINES(j, Bs.n) {
+        double s = 0.0, sd = 0.0, sa = 0.0;
+        if (live) {
+            for (int p = __ldg(Bs.cs + j); p < __ldg(Bs.cs + j + 1); ++p) {
+                const double a = __ldg(Bs.cv + p);
+                const size_t qi = (size_t)__ldg(Bs.ri + p) * V.Kp + k;
+                const double dv = V.dray[qi];
+                s = fma(a, M.yh[qi] + (double)M.ya[qi], s);
+                sd = fma(a, dv, sd);
+                sa = fma(fabs(a), fabs(dv), sa);
+            }
+            const size_t q = (size_t)j * V.Kp + k;
+            M.atyf[q] = s;
+            acc.add_b(O, (int)j, s, M.xh[q] + (double)M.xa[q], V.olo[q], V.ohi[q]);
+            ray.add_col_b(O, (int)j, sd, sa, V.olo[q], V.ohi[q]);
+        }
+    }
+    const double vmax = lanes_reduce(acc.vmax, sm, OpMax());
+    const double dres = lanes_reduce(acc.dres, sm, OpSum());
+    const double pobj = lanes_reduce(acc.pobj, sm, OpSum());
+    const double dobj = lanes_reduce(acc.dobj, sm, OpSum());
+    const double bad = lanes_reduce(acc.bad, sm, OpSum());
+    const double rl = lanes_reduce(ray.l, sm, OpSum());
+    const double rcs = lanes_reduce(ray.cscale, sm, OpSum());
+    const double rci = lanes_reduce(ray.cinf, sm, OpSum());
+    if ((threadIdx.x >> 5) == 0 && k < V.K) {
+        var_partial(V, SLOT_COL_MAX, k)[blockIdx.x] = vmax;
+        var_partial(V, SLOT_COL_DRES, k)[blockIdx.x] = dres;
+        var_partial(V, SLOT_COL_POBJ, k)[blockIdx.x] = pobj;
+        var_partial(V, SLOT_COL_DOBJ, k)[blockIdx.x] = dobj;
+        var_partial(V, SLOT_B, k)[blockIdx.x] = bad;
+        var_partial(V, SLOT_RAY_L, k)[blockIdx.x] = rl;
+        var_partial(V, SLOT_RAY_CSCALE, k)[blockIdx.x] = rcs;
+        var_partial(V, SLOT_RAY_CINF, k)[blockIdx.x] = rci;
+    }
+}
+
+// Restart of a variant to its average: its base moves there and its
+// correction LP is rebuilt from the residual pass's FP64 products
+// (k_recenter_mx per variant).  `force` rebuilds every running variant.
+__global__ void __launch_bounds__(kBlock) kvm_recenter(int m, int n, VarRefs V, VarMixed M, int force) {
+    const int k = blockIdx.y * 32 + (threadIdx.x & 31);
+    if (k >= V.K) return;
+    const DevState& s = V.st[k];
+    if (s.done || (!force && !s.restart_pending)) return;
+    const float inf = __int_as_float(0x7f800000);
+    MC_VARIANT_LINES(l, (long long)n + m) {
+        if (l < n) {
+            const size_t q = (size_t)l * V.Kp + k;
+            const double xh = M.xh[q] + (double)M.xa[q];
+            M.xh[q] = xh;
+            M.x[q] = 0.f;
+            M.xa[q] = 0.f;
+            M.g[q] = (float)(M.c64[l] + M.atyf[q]);
+            const double lo = V.lo[q], hi = V.hi[q];
+            M.lo[q] = (lo <= -1e299) ? -inf : (float)(lo - xh);
+            M.hi[q] = (hi >= 1e299) ? inf : (float)(hi - xh);
+        } else {
+            const long long i = l - n;
+            const size_t q = (size_t)i * V.Kp + k;
+            const double yh = M.yh[q] + (double)M.ya[q];
+            M.yh[q] = yh;
+            M.y[q] = 0.f;
+            M.ya[q] = 0.f;
+            M.yb[q] = (float)yh;
+            const double ax = M.axf[q], lo = M.blo64[i], hi = M.bhi64[i];
+            M.rlo[q] = (lo <= -1e299) ? inf : (float)(ax - lo);
+            M.rhi[q] = (hi >= 1e299) ? -inf : (float)(ax - hi);
+        }
+    }
+}
+
+// unscaled outputs of the FP32 form: x = (xh + dx_avg) D_C, y = (yh + dy_avg) D_R
+// (the ray for a variant proven infeasible by one)
+__global__ void __launch_bounds__(kBlock) kvm_unscale_out(int m, int n, VarRefs V, VarMixed M,
+                                                          const double* __restrict__ col_scale,
+                                                          const double* __restrict__ row_scale,
+                                                          double* __restrict__ xo, double* __restrict__ yo) {
+    const int k = blockIdx.y * 32 + (threadIdx.x & 31);
+    if (k >= V.K) return;
+    const bool ray = V.st[k].status == 2 && V.st[k].cert == MC_CERT_DUAL_RAY;
+    MC_VARIANT_LINES(l, (long long)n + m) {
+        if (l < n) {
+            const size_t q = (size_t)l * V.Kp + k;
+            xo[(size_t)k * n + l] = __dmul_rn(M.xh[q] + (double)M.xa[q], col_scale[l]);
+        } else {
+            const long long i = l - n;
+            const size_t q = (size_t)i * V.Kp + k;
+            const double yv = ray ? V.dray[q] : M.yh[q] + (double)M.ya[q];
+            yo[(size_t)k * m + i] = __dmul_rn(yv, row_scale[i]);
+        }
+    }
+}
+
+struct EngineVariantsMixed {
+    VarBase Bs;
+    VarRefs V;
+    VarMixed M;
+    Original O;
+    dim3 grid;
+    int shape_class(const DevState&) const { return 0; }
+    void use_class(int) const {}
+
+    int iteration(Ctx& ctx, int k, bool step, const Controls& ctl) const {
+        cudaStream_t s = ctx.stream;
+        ctx.begin_launch(MC_KERNEL_PRIMAL);
+        if (step) kvm_primal<true><<<grid, kBlock, 0, s>>>(Bs.n, V, M, k);
+        else kvm_primal<false><<<grid, kBlock, 0, s>>>(Bs.n, V, M, k);
+        ctx.end_launch();
+        if (step) {
+            ctx.begin_launch(MC_KERNEL_DUAL_STEP);
+            kvm_dual_probe<<<grid, kBlock, 0, s>>>(Bs.m, V, M);
+            ctx.end_launch();
+            ctx.begin_launch(MC_KERNEL_OTHER);
+            kv_step_size<<<V.K, 256, 0, s>>>(V, ctl);
+            ctx.end_launch();
+            ctx.begin_launch(MC_KERNEL_DUAL_STEP);
+            kvm_dual_apply<<<grid, kBlock, 0, s>>>(Bs.m, V, M, k);
+            ctx.end_launch();
+        } else {
+            ctx.begin_launch(MC_KERNEL_DUAL);
+            kvm_dual<<<grid, kBlock, 0, s>>>(Bs.m, V, M, k);
+            ctx.end_launch();
+        }
+        return ctx.launch_check("variant iteration (FP32)");
+    }
+
+    int residual_pass(Ctx& ctx) const {
+        ctx.begin_launch(MC_KERNEL_RESIDUAL);
+        kvm_residual_rows<<<grid, kBlock, 0, ctx.stream>>>(Bs, V, M, O);
+        ctx.end_launch();
+        ctx.begin_launch(MC_KERNEL_RESIDUAL);
+        kvm_residual_cols<<<grid, kBlock, 0, ctx.stream>>>(Bs, V, M, O);
+        ctx.end_launch();
+        return ctx.launch_check("variant residual (FP32)");
+    }
+
+    int recenter(Ctx& ctx, int force) const {
+        ctx.begin_launch(MC_KERNEL_OTHER);
+        kvm_recenter<<<grid, kBlock, 0, ctx.stream>>>(Bs.m, Bs.n, V, M, force);
+        ctx.end_launch();
+        return ctx.launch_check("variant recenter");
+    }
+
+    int check(Ctx& ctx, long long span, int final_pass, const Controls& ctl, const TraceBuf&) const {
+        TRY(residual_pass(ctx));
+        ctx.begin_launch(MC_KERNEL_RESIDUAL);
+        kv_finalize<<<V.K, 256, 0, ctx.stream>>>(V, O.offset, span, final_pass, ctl);
+        ctx.end_launch();
+        if (!final_pass) TRY(recenter(ctx, 0));
+        ctx.begin_launch(MC_KERNEL_OTHER);
+        kv_poll<<<1, 1024, 0, ctx.stream>>>(V);
+        ctx.end_launch();
+        return ctx.launch_check("variant check (FP32)");
+    }
+};
+
 // Host driver: the base LP's setup as a single solve's (upload, validation,
 // transpose, Ruiz, norms), then the variants' bounds, starts and
 // certificates, the PDHG loop in chunk graphs, and per-variant outputs.
@@ -650,8 +1031,7 @@ int solve_variants(Ctx& ctx, const mc_lp* base, int count, const double* const* 
     if (!base || count <= 0 || !results) return set_error(MC_ERR_INVALID_ARGUMENT, "no variants");
     TRY(validate_options(o));
     TRY(validate_lp(base));
-    if (o->precision != MC_PRECISION_FP64)
-        return set_error(MC_ERR_INVALID_ARGUMENT, "variant solves run in FP64");
+    const bool mixed = o->precision == MC_PRECISION_FP32_REFINE;
     const int m = base->num_rows, n = base->num_cols;
     const long long nnz = base->nnz;
     for (int b = 0; b < count; ++b) {
@@ -720,6 +1100,17 @@ int solve_variants(Ctx& ctx, const mc_lp* base, int count, const double* const* 
     const size_t o_wy = any_wy ? L.add<double>((long long)count * m) : 0;
     const size_t o_hw = L.add<int>(2LL * count);
     const size_t o_xo = L.add<double>((long long)count * n), o_yo = L.add<double>((long long)count * m);
+    // FP32 form: FP32 matrix copies and norms, FP32 variant-minor correction data
+    size_t o_f_cv = 0, o_f_rv = 0, o_f_cn = 0, o_f_rn = 0, o_fn[7] = {}, o_fxdx = 0, o_fm[6] = {};
+    if (mixed) {
+        o_f_cv = L.add<float>(nnz + 16);
+        o_f_rv = L.add<float>(nnz + 16);
+        o_f_cn = L.add<float>(n);
+        o_f_rn = L.add<float>(m);
+        for (auto& v : o_fn) v = L.add<float>(nk);
+        o_fxdx = L.add<float>(2 * nk);
+        for (auto& v : o_fm) v = L.add<float>(mk);
+    }
     TRY(ctx.arena.reserve(L.offset));
     char* A = static_cast<char*>(ctx.arena.base);
     auto at = [&](size_t off) { return static_cast<void*>(A + off); };
@@ -871,20 +1262,88 @@ int solve_variants(Ctx& ctx, const mc_lp* base, int count, const double* const* 
                  o->primal_weight_smoothing, o->restart_every, o->restart_strategy, o->adaptive_step_size,
                  o->adaptive_primal_weight};
     TraceBuf tr{0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-    EngineVariants eng;
-    eng.Bs = Bs;
-    eng.V = V;
-    eng.O = O;
-    eng.grid = grid;
-    TRY(run_chunks(ctx, eng, V.global, o->max_iterations, o->restart_every,
-                   o->check_every_chunks > 0 ? o->check_every_chunks : 1, ctl, tr));
+    const int poll_every = o->check_every_chunks > 0 ? o->check_every_chunks : 1;
+    VarMixed M{};
+    if (!mixed) {
+        EngineVariants eng;
+        eng.Bs = Bs;
+        eng.V = V;
+        eng.O = O;
+        eng.grid = grid;
+        TRY(run_chunks(ctx, eng, V.global, o->max_iterations, o->restart_every, poll_every, ctl, tr));
+    } else {
+        float* f_cv = static_cast<float*>(at(o_f_cv));
+        float* f_rv = static_cast<float*>(at(o_f_rv));
+        float* f_cn = static_cast<float*>(at(o_f_cn));
+        float* f_rn = static_cast<float*>(at(o_f_rn));
+        const int nbz = blocks_for(ctx, nnz + 16, kBlock) * 4;
+        ctx.begin_launch(MC_KERNEL_SETUP);
+        k_to_float<<<nbz, kBlock, 0, s>>>(nnz + 16, cv, f_cv);
+        ctx.end_launch();
+        ctx.begin_launch(MC_KERNEL_SETUP);
+        k_to_float<<<nbz, kBlock, 0, s>>>(nnz + 16, rv, f_rv);
+        ctx.end_launch();
+        ctx.begin_launch(MC_KERNEL_SETUP);
+        k_to_float<<<blocks_for(ctx, n, kBlock), kBlock, 0, s>>>(n, col_norm, f_cn);
+        ctx.end_launch();
+        ctx.begin_launch(MC_KERNEL_SETUP);
+        k_to_float<<<blocks_for(ctx, m, kBlock), kBlock, 0, s>>>(m, row_norm, f_rn);
+        ctx.end_launch();
+        M.cs = cs;
+        M.ri = ri;
+        M.cv = f_cv;
+        M.rs = rs;
+        M.ci = ci;
+        M.rv = f_rv;
+        M.col_norm = f_cn;
+        M.row_norm = f_rn;
+        M.c64 = c;
+        M.blo64 = blo;
+        M.bhi64 = bhi;
+        M.xh = V.x;       // the FP64 start point is every variant's first base
+        M.yh = V.y;
+        M.axf = V.axb;
+        M.atyf = V.xb;
+        float* fn[7];
+        for (int q = 0; q < 7; ++q) fn[q] = static_cast<float*>(at(o_fn[q]));
+        float* fm[6];
+        for (int q = 0; q < 6; ++q) fm[q] = static_cast<float*>(at(o_fm[q]));
+        M.x = fn[0];
+        M.xb = fn[1];
+        M.xa = fn[2];
+        M.g = fn[3];
+        M.lo = fn[4];
+        M.hi = fn[5];
+        M.xdx = static_cast<float*>(at(o_fxdx));
+        M.y = fm[0];
+        M.ya = fm[1];
+        M.axb = fm[2];
+        M.yb = fm[3];
+        M.rlo = fm[4];
+        M.rhi = fm[5];
+        // corrections start at zero (padding lanes included: gathers read them)
+        for (int q = 0; q < 7; ++q) CU(cudaMemsetAsync(fn[q], 0, sizeof(float) * (size_t)nk, s));
+        CU(cudaMemsetAsync(M.xdx, 0, sizeof(float) * 2 * (size_t)nk, s));
+        for (int q = 0; q < 6; ++q) CU(cudaMemsetAsync(fm[q], 0, sizeof(float) * (size_t)mk, s));
+        EngineVariantsMixed eng;
+        eng.Bs = Bs;
+        eng.V = V;
+        eng.M = M;
+        eng.O = O;
+        eng.grid = grid;
+        // the first correction LP of every running variant, around its start
+        TRY(eng.residual_pass(ctx));
+        TRY(eng.recenter(ctx, 1));
+        TRY(run_chunks(ctx, eng, V.global, o->max_iterations, o->restart_every, poll_every, ctl, tr));
+    }
     CU(cudaEventRecord(ctx.ev_c, s));
 
     // ---- outputs
     double* xo = static_cast<double*>(at(o_xo));
     double* yo = static_cast<double*>(at(o_yo));
     ctx.begin_launch(MC_KERNEL_OTHER);
-    kv_unscale_out<<<grid, kBlock, 0, s>>>(Bs, V, col_scale, row_scale, xo, yo);
+    if (mixed) kvm_unscale_out<<<grid, kBlock, 0, s>>>(m, n, V, M, col_scale, row_scale, xo, yo);
+    else kv_unscale_out<<<grid, kBlock, 0, s>>>(Bs, V, col_scale, row_scale, xo, yo);
     ctx.end_launch();
     TRY(ctx.launch_check("variant unscale"));
     for (int b = 0; b < count; ++b) {
@@ -935,6 +1394,8 @@ int solve_variants(Ctx& ctx, const mc_lp* base, int count, const double* const* 
         r.final_primal_weight = S.omega;
         r.final_step_size = S.eta;
         r.kernel_launches = total;
+        r.refinement_rounds = mixed ? S.restarts : 0;  // each restart re-centres the variant's FP64 base
+        r.inner_iterations = mixed ? S.iter : 0;
         for (int q = 0; q < MC_KERNEL_KINDS; ++q) {
             r.launches_by_kind[q] = ctx.launches[q];
             r.kernel_ms_by_kind[q] = ctx.kernel_ms[q];

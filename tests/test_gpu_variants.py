@@ -15,7 +15,7 @@ import pytest
 
 from certificates import check_certificate
 from conftest import options, rel
-from mcpdlp import PdlpOptions, PdlpStatus, generators
+from mcpdlp import PdlpOptions, PdlpStatus, Precision, generators
 
 pytestmark = pytest.mark.gpu
 
@@ -31,11 +31,12 @@ def node_round(seed: int, count: int, m=300, n=900):
     return base, variants
 
 
-def test_variants_match_solo_solves_and_the_batch(gpu_ctx, oracle):
+@pytest.mark.parametrize("precision", [Precision.fp64, Precision.fp32_refine])
+def test_variants_match_solo_solves_and_the_batch(gpu_ctx, oracle, precision):
     base, variants = node_round(3, 37)   # not a multiple of 32: a partly filled warp
     res = gpu_ctx.solve_variants(base, [v.var_lower for v in variants], [v.var_upper for v in variants],
-                                 opts(1e-8))
-    batch = gpu_ctx.solve_batch(variants, opts(1e-8))
+                                 opts(1e-8, precision=precision))
+    batch = gpu_ctx.solve_batch(variants, opts(1e-8, precision=precision))
     assert len(res) == len(variants)
     optimal = 0
     for v, r, b in zip(variants, res, batch):
@@ -67,17 +68,19 @@ def test_base_bounds_variant_is_the_base_lp(gpu_ctx, oracle):
     assert rel(res[0].objective, base.info["optimum"]) <= 1e-6
 
 
-def test_variants_deterministic_and_warm_started(gpu_ctx):
+@pytest.mark.parametrize("precision", [Precision.fp64, Precision.fp32_refine])
+def test_variants_deterministic_and_warm_started(gpu_ctx, precision):
     base, variants = node_round(5, 12)
     lows, ups = [v.var_lower for v in variants], [v.var_upper for v in variants]
-    a = gpu_ctx.solve_variants(base, lows, ups, opts(1e-8))
-    b = gpu_ctx.solve_variants(base, lows, ups, opts(1e-8))
+    a = gpu_ctx.solve_variants(base, lows, ups, opts(1e-8, precision=precision))
+    b = gpu_ctx.solve_variants(base, lows, ups, opts(1e-8, precision=precision))
     for x, y in zip(a, b):
         assert x.status == y.status and x.iterations == y.iterations and x.objective == y.objective
         assert np.array_equal(x.primal, y.primal) and np.array_equal(x.dual, y.dual)
     starts_x = [r.primal if r.status == PdlpStatus.optimal else None for r in a]
     starts_y = [r.dual if r.status == PdlpStatus.optimal else None for r in a]
-    w = gpu_ctx.solve_variants(base, lows, ups, opts(1e-8), initial_primal=starts_x, initial_dual=starts_y)
+    w = gpu_ctx.solve_variants(base, lows, ups, opts(1e-8, precision=precision), initial_primal=starts_x,
+                               initial_dual=starts_y)
     for cold, warm in zip(a, w):
         assert warm.status == cold.status
         if cold.status == PdlpStatus.optimal:
@@ -85,14 +88,16 @@ def test_variants_deterministic_and_warm_started(gpu_ctx):
             assert rel(warm.objective, cold.objective) <= 1e-7
 
 
-def test_infeasible_variants_are_certified(gpu_ctx):
+@pytest.mark.parametrize("precision", [Precision.fp64, Precision.fp32_refine])
+def test_infeasible_variants_are_certified(gpu_ctx, precision):
     base, variants = node_round(6, 40)
     # and the base with one crossed pair of bounds (column 3 only)
     crossed = base.copy()
     crossed.var_lower = crossed.var_lower.copy()
     crossed.var_lower[3] = crossed.var_upper[3] + 0.5
     vs = variants + [crossed]
-    res = gpu_ctx.solve_variants(base, [v.var_lower for v in vs], [v.var_upper for v in vs], opts(1e-6))
+    res = gpu_ctx.solve_variants(base, [v.var_lower for v in vs], [v.var_upper for v in vs],
+                                 opts(1e-6, precision=precision))
     kinds = set()
     for v, r in zip(vs, res):
         if r.status == PdlpStatus.infeasible_or_unbounded:
@@ -103,11 +108,7 @@ def test_infeasible_variants_are_certified(gpu_ctx):
     assert res[-1].extra["certificate"] == "crossed_bounds" and res[-1].extra["certificate_index"] == 3
 
 
-def test_variants_options_rejected(gpu_ctx):
-    from mcpdlp import Precision
+def test_variants_bad_arrays_rejected(gpu_ctx):
     base, variants = node_round(7, 2)
-    with pytest.raises(ValueError):
-        gpu_ctx.solve_variants(base, [variants[0].var_lower], [variants[0].var_upper],
-                               opts(1e-6, precision=Precision.fp32_refine))
     with pytest.raises(ValueError):
         gpu_ctx.solve_variants(base, [variants[0].var_lower[:-1]], [variants[0].var_upper], opts(1e-6))
