@@ -455,7 +455,8 @@ __global__ void kv_poll(VarRefs V) {
 // arrays: scaled and sentinel forms, the crossed-bound certificate, and the
 // start x = proj(given start or 0) (pdlp.cpp:186-191).  Padding lanes get
 // zeros, so that gathers over them read finite values.
-__global__ void __launch_bounds__(kBlock) kv_setup_cols(VarBase Bs, VarRefs V, const double* __restrict__ lo_in,
+__global__ void __launch_bounds__(kBlock) kv_setup_cols(VarBase Bs, VarRefs V, const int* __restrict__ perm,
+                                                        const double* __restrict__ lo_in,
                                                         const double* __restrict__ hi_in,
                                                         const double* __restrict__ warm_x,
                                                         const int* __restrict__ has_warm_x,
@@ -470,7 +471,8 @@ __global__ void __launch_bounds__(kBlock) kv_setup_cols(VarBase Bs, VarRefs V, c
             V.xdx[2 * q] = V.xdx[2 * q + 1] = 0.0;
             continue;
         }
-        const size_t g = (size_t)k * Bs.n + j;
+        const int b = perm[k];  // the caller's variant in slot k
+        const size_t g = (size_t)b * Bs.n + j;
         const double s = col_scale[j];
         const double inv = 1.0 / s;
         const double l0 = lo_in[g], h0 = hi_in[g];
@@ -486,7 +488,7 @@ __global__ void __launch_bounds__(kBlock) kv_setup_cols(VarBase Bs, VarRefs V, c
             atomicOr(V.flags + k, 1);
             atomicMin(V.cert_idx + k, (int)j);
         }
-        const double start = (has_warm_x && has_warm_x[k]) ? __dmul_rn(warm_x[g], inv) : 0.0;
+        const double start = (has_warm_x && has_warm_x[b]) ? __dmul_rn(warm_x[g], inv) : 0.0;
         const double x0 = clampv(start, lsent, hsent);
         V.x[q] = x0;
         V.xa[q] = x0;
@@ -498,7 +500,8 @@ __global__ void __launch_bounds__(kBlock) kv_setup_cols(VarBase Bs, VarRefs V, c
 
 // Row-activity certificate per variant (the packed batch's kb_setup_rows
 // test on the variant's box) and the dual start.
-__global__ void __launch_bounds__(kBlock) kv_setup_rows(VarBase Bs, VarRefs V, const double* __restrict__ rlo_in,
+__global__ void __launch_bounds__(kBlock) kv_setup_rows(VarBase Bs, VarRefs V, const int* __restrict__ perm,
+                                                        const double* __restrict__ rlo_in,
                                                         const double* __restrict__ rhi_in,
                                                         const double* __restrict__ row_scale,
                                                         const double* __restrict__ col_scale,
@@ -532,7 +535,8 @@ __global__ void __launch_bounds__(kBlock) kv_setup_rows(VarBase Bs, VarRefs V, c
             atomicOr(V.flags + k, 2);
             atomicMin(V.cert_idx + V.K + k, (int)i);
         }
-        const double y0 = (has_warm_y && has_warm_y[k]) ? __dmul_rn(warm_y[(size_t)k * Bs.m + i], 1.0 / s) : 0.0;
+        const int b = perm[k];
+        const double y0 = (has_warm_y && has_warm_y[b]) ? __dmul_rn(warm_y[(size_t)b * Bs.m + i], 1.0 / s) : 0.0;
         V.y[q] = y0;
         V.ya[q] = y0;
         V.axb[q] = 0.0;
@@ -1099,6 +1103,7 @@ int solve_variants(Ctx& ctx, const mc_lp* base, int count, const double* const* 
     const size_t o_wx = any_wx ? L.add<double>((long long)count * n) : 0;
     const size_t o_wy = any_wy ? L.add<double>((long long)count * m) : 0;
     const size_t o_hw = L.add<int>(2LL * count);
+    const size_t o_perm = L.add<int>(count);
     const size_t o_xo = L.add<double>((long long)count * n), o_yo = L.add<double>((long long)count * m);
     // FP32 form: FP32 matrix copies and norms, FP32 variant-minor correction data
     size_t o_f_cv = 0, o_f_rv = 0, o_f_cn = 0, o_f_rn = 0, o_fn[7] = {}, o_fxdx = 0, o_fm[6] = {};
@@ -1238,17 +1243,46 @@ int solve_variants(Ctx& ctx, const mc_lp* base, int count, const double* const* 
     V.partials = static_cast<double*>(at(o_vpart));
     V.flags = static_cast<int*>(at(o_flags));
     V.cert_idx = static_cast<int*>(at(o_cert));
-    CU(cudaMemsetAsync(V.flags, 0, sizeof(int) * count, s));
-    CU(cudaMemsetAsync(V.cert_idx, 0x7f, sizeof(int) * 2 * (size_t)count, s));  // "none" above any index
     CU(cudaMemsetAsync(V.partials, 0, sizeof(double) * (size_t)NUM_SLOTS * Kp * nbx, s));
     const dim3 grid((unsigned)nbx, (unsigned)groups);
-    ctx.begin_launch(MC_KERNEL_SETUP);
-    kv_setup_cols<<<grid, kBlock, 0, s>>>(Bs, V, lo_in, hi_in, wx, any_wx ? has_warm : nullptr, col_scale);
-    ctx.end_launch();
-    ctx.begin_launch(MC_KERNEL_SETUP);
-    kv_setup_rows<<<grid, kBlock, 0, s>>>(Bs, V, rlo_in, rhi_in, row_scale, col_scale, wy,
-                                          any_wy ? has_warm + count : nullptr);
-    ctx.end_launch();
+    // Slots: variant b of the caller sits in slot k with perm[k] = b.  The
+    // variants certified infeasible at setup go last, so that the groups of
+    // 32 slots that hold only finished variants leave every kernel at once;
+    // the certificates are found with the identity order first.
+    int* perm_dev = static_cast<int*>(at(o_perm));
+    std::vector<int> perm(count);
+    for (int b = 0; b < count; ++b) perm[b] = b;
+    auto setup_slots = [&]() -> int {
+        CU(cudaMemcpyAsync(perm_dev, perm.data(), sizeof(int) * count, cudaMemcpyHostToDevice, s));
+        CU(cudaMemsetAsync(V.flags, 0, sizeof(int) * count, s));
+        CU(cudaMemsetAsync(V.cert_idx, 0x7f, sizeof(int) * 2 * (size_t)count, s));  // "none" above any index
+        ctx.begin_launch(MC_KERNEL_SETUP);
+        kv_setup_cols<<<grid, kBlock, 0, s>>>(Bs, V, perm_dev, lo_in, hi_in, wx, any_wx ? has_warm : nullptr,
+                                              col_scale);
+        ctx.end_launch();
+        ctx.begin_launch(MC_KERNEL_SETUP);
+        kv_setup_rows<<<grid, kBlock, 0, s>>>(Bs, V, perm_dev, rlo_in, rhi_in, row_scale, col_scale, wy,
+                                              any_wy ? has_warm + count : nullptr);
+        ctx.end_launch();
+        return ctx.launch_check("variant slots");
+    };
+    TRY(setup_slots());
+    {
+        std::vector<int> hflags(count);
+        CU(cudaMemcpyAsync(hflags.data(), V.flags, sizeof(int) * count, cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        TRY(ctx.drain_profile());
+        std::vector<int> order;
+        order.reserve(count);
+        for (int b = 0; b < count; ++b)
+            if (!hflags[b]) order.push_back(b);
+        for (int b = 0; b < count; ++b)
+            if (hflags[b]) order.push_back(b);
+        if (order != perm) {
+            perm = order;
+            TRY(setup_slots());
+        }
+    }
     ctx.begin_launch(MC_KERNEL_SETUP);
     kv_setup_state<<<(count + 255) / 256, 256, 0, s>>>(V, st);
     ctx.end_launch();
@@ -1346,11 +1380,12 @@ int solve_variants(Ctx& ctx, const mc_lp* base, int count, const double* const* 
     else kv_unscale_out<<<grid, kBlock, 0, s>>>(Bs, V, col_scale, row_scale, xo, yo);
     ctx.end_launch();
     TRY(ctx.launch_check("variant unscale"));
-    for (int b = 0; b < count; ++b) {
+    for (int k = 0; k < count; ++k) {
+        const int b = perm[k];
         if (x_out && x_out[b])
-            CU(cudaMemcpyAsync(x_out[b], xo + (size_t)b * n, sizeof(double) * n, cudaMemcpyDefault, s));
+            CU(cudaMemcpyAsync(x_out[b], xo + (size_t)k * n, sizeof(double) * n, cudaMemcpyDefault, s));
         if (y_out && y_out[b])
-            CU(cudaMemcpyAsync(y_out[b], yo + (size_t)b * m, sizeof(double) * m, cudaMemcpyDefault, s));
+            CU(cudaMemcpyAsync(y_out[b], yo + (size_t)k * m, sizeof(double) * m, cudaMemcpyDefault, s));
     }
     std::vector<DevState> hs(count + 2);
     CU(cudaMemcpyAsync(hs.data(), st, sizeof(DevState) * (count + 2), cudaMemcpyDeviceToHost, s));
@@ -1366,9 +1401,10 @@ int solve_variants(Ctx& ctx, const mc_lp* base, int count, const double* const* 
     long long total = 0;
     for (int q = 0; q < MC_KERNEL_KINDS; ++q) total += ctx.launches[q];
     const double total_ms = now_ms() - t_begin;
-    for (int b = 0; b < count; ++b) {
+    for (int k = 0; k < count; ++k) {
+        const int b = perm[k];
         mc_pdlp_result& r = results[b];
-        const DevState& S = hs[2 + b];
+        const DevState& S = hs[2 + k];
         r.status = S.status;
         r.objective = S.objective;
         r.primal_infeasibility = S.primal_infeas;
@@ -1376,8 +1412,8 @@ int solve_variants(Ctx& ctx, const mc_lp* base, int count, const double* const* 
         r.duality_gap = S.gap;
         r.iterations = S.iter;
         r.certificate = S.status == MC_PDLP_INFEASIBLE_OR_UNBOUNDED ? S.cert : MC_CERT_NONE;
-        r.certificate_index = r.certificate == MC_CERT_CROSSED_BOUNDS ? hcert[b]
-                              : r.certificate == MC_CERT_ROW_ACTIVITY ? hcert[count + b]
+        r.certificate_index = r.certificate == MC_CERT_CROSSED_BOUNDS ? hcert[k]
+                              : r.certificate == MC_CERT_ROW_ACTIVITY ? hcert[count + k]
                                                                       : -1;
         fill_message(&r, S.status == MC_PDLP_OPTIMAL ? "PDLP converged"
                          : r.certificate == MC_CERT_CROSSED_BOUNDS ? "infeasible: crossed variable bounds"
