@@ -211,8 +211,9 @@ int mc_pdlp_abi_version(void);
 void mc_pdlp_default_options(mc_pdlp_options* options);
 
 /* sizeof of mc_lp, mc_pdlp_options, mc_pdlp_result, mc_pdlp_trace,
- * mc_verify_report (in that order) into sizes[0..count-1]; lets bindings
- * check their struct layouts. */
+ * mc_verify_report, mc_canonical_lp, mc_presolve_options, mc_presolve_info
+ * (in that order) into sizes[0..count-1]; lets bindings check their struct
+ * layouts. */
 int mc_pdlp_struct_sizes(size_t* sizes, int count);
 
 /* Thread-local text of the last failure ("" if none). Returns MC_OK. */
@@ -503,6 +504,113 @@ int mc_ruiz_equilibrate_noalloc(int32_t m, int32_t n, int64_t nnz, const int32_t
                                 double* var_upper, double* row_lower, double* row_upper,
                                 int64_t max_iterations, double* row_scale, double* col_scale,
                                 int64_t* iterations_executed, void* stream);
+
+/*
+ * Presolve of a canonical model on the device: presolve() and postsolve() at
+ * src/presolve/presolve.cpp:20-217 and :219-317 (options and statistics:
+ * include/markov_cero/presolve/presolve.hpp:12-36; the record stack:
+ * include/markov_cero/presolve/presolve_stack.hpp:9-72).
+ *
+ * The canonical model is SparseCanonicalModel (min c.x + offset, A x = rhs,
+ * x >= 0; include/markov_cero/transform/sparse_canonical_model.hpp:12-19):
+ * CSC with strictly increasing row indices in each column, no explicit zeros,
+ * finite values, rhs and objective.  A model that breaks these is
+ * MC_ERR_INVALID_ARGUMENT (the reference's validate() throws).  The
+ * reference's dense-simplex size cap (4096 rows and columns, 4Mi nonzeros,
+ * src/linalg/sparse_basis.cpp:26-34) is not applied: the device presolve
+ * takes any model within the int32 index range.
+ *
+ * Each pass removes empty rows (row order), then empty columns (column
+ * order), then row singletons in row order, each fixing its variable and
+ * substituting it into the other rows -- with exactly the reference's
+ * sequential semantics: a row left with one entry by an earlier singleton of
+ * the same pass is itself a singleton, and right-hand sides are updated in
+ * the reference's order, so the reduced model, the record stack and the maps
+ * are bit-identical to the reference's.  Up to max_passes passes; stops after
+ * a pass without reductions.
+ *
+ * Arrays of mc_canonical_lp may be host or device memory (cudaMemcpyDefault).
+ */
+typedef struct mc_canonical_lp {
+    int32_t num_rows, num_cols;
+    int64_t nnz;
+    const int32_t* col_start; /* [num_cols + 1] */
+    const int32_t* row_index; /* [nnz] */
+    const double* value;      /* [nnz] */
+    const double* rhs;        /* [num_rows] */
+    const double* objective;  /* [num_cols] */
+    double objective_offset;
+} mc_canonical_lp;
+
+typedef struct mc_presolve_options { /* PresolveOptions, presolve.hpp:12-17 */
+    int64_t max_passes;              /* 5 */
+    double feasibility_tolerance;    /* 1e-9 */
+    double dual_tolerance;           /* 1e-9 */
+    double pivot_tolerance;          /* 1e-12 */
+} mc_presolve_options;
+
+void mc_presolve_default_options(mc_presolve_options* options);
+
+/* lp::reference::SolveStatus values that presolve returns */
+typedef enum mc_presolve_status {
+    MC_PRESOLVE_OPTIMAL = 0,    /* reduced ("presolve complete") */
+    MC_PRESOLVE_INFEASIBLE = 1, /* an empty row with a non-zero rhs, or a negative singleton value */
+    MC_PRESOLVE_UNBOUNDED = 2   /* an empty column with a negative cost */
+} mc_presolve_status;
+
+/* ReductionRecord alternatives, in the variant's order (presolve_stack.hpp:38-39) */
+typedef enum mc_record_kind {
+    MC_RECORD_EMPTY_ROW = 0,      /* index = row, value = rhs_value */
+    MC_RECORD_EMPTY_COLUMN = 1,   /* index = column, value = objective_coeff, value2 = fixed_value */
+    MC_RECORD_FIXED_VARIABLE = 2, /* index = column, value = fixed_value, value2 = objective_coeff;
+                                     incident rows and coefficients */
+    MC_RECORD_ROW_SINGLETON = 3   /* index = row, variable = column, value = coefficient, value2 = rhs_value */
+} mc_record_kind;
+
+typedef struct mc_presolve_info {
+    int32_t status; /* mc_presolve_status */
+    char message[96];
+    /* PresolveStatistics, presolve.hpp:19-29 */
+    int64_t passes_executed, empty_rows_removed, empty_cols_removed, fixed_vars_removed, row_singletons_removed;
+    int64_t original_rows, original_cols, presolved_rows, presolved_cols;
+    int64_t presolved_nnz;
+    double objective_offset; /* of the reduced model */
+    int64_t records;          /* stack size */
+    int64_t incident_entries; /* rows over all fixed-variable records */
+    int64_t scan_rounds;      /* device rounds of the singleton scans, over all passes */
+    double presolve_ms;       /* host wall time of mc_presolve_run */
+} mc_presolve_info;
+
+typedef struct mc_presolve mc_presolve; /* a presolve's result, held in device memory */
+
+/* Runs presolve on the context's device; *out receives the result (status
+ * infeasible/unbounded are results, not errors).  Free with mc_presolve_free. */
+int mc_presolve_run(mc_pdlp_ctx* ctx, const mc_canonical_lp* lp, const mc_presolve_options* options,
+                    mc_presolve** out);
+int mc_presolve_get_info(const mc_presolve* p, mc_presolve_info* info);
+/* The reduced model (presolved_rows x presolved_cols, presolved_nnz): host or
+ * device destinations; any pointer may be NULL.  Empty when status is not
+ * optimal (the reference returns a default model then). */
+int mc_presolve_get_model(const mc_presolve* p, int32_t* col_start, int32_t* row_index, double* value,
+                          double* rhs, double* objective);
+/* presolved_to_original rows [presolved_rows] and columns [presolved_cols] */
+int mc_presolve_get_maps(const mc_presolve* p, int64_t* row_map, int64_t* col_map);
+/* The stack, oldest first: kind, index, variable (-1 if none), value, value2
+ * [records]; incident_start [records + 1] into incident_row and
+ * incident_coefficient [incident_entries].  Any pointer may be NULL. */
+int mc_presolve_get_records(const mc_presolve* p, int32_t* kind, int64_t* index, int64_t* variable, double* value,
+                            double* value2, int64_t* incident_start, int64_t* incident_row,
+                            double* incident_coefficient);
+/* postsolve() against the model presolve ran on: reduced_primal
+ * [reduced_cols] and reduced_dual [reduced_rows] (entries past a shorter
+ * array count as missing, as in the reference); writes primal [num_cols],
+ * dual [num_rows] and the objective.  The singleton duals and the objective
+ * are summed in double-double arithmetic where the reference uses long
+ * double.  A non-finite dual or objective is MC_ERR_INVALID_ARGUMENT (the
+ * reference throws overflow_error). */
+int mc_postsolve(mc_pdlp_ctx* ctx, const mc_presolve* p, const double* reduced_primal, int64_t reduced_cols,
+                 const double* reduced_dual, int64_t reduced_rows, double* primal, double* dual, double* objective);
+void mc_presolve_free(mc_presolve* p);
 
 #ifdef __cplusplus
 }

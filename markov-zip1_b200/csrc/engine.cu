@@ -187,6 +187,7 @@ int pick_lanes(double mean_len) {
 #include "variants.cuh"
 #include "kernel_api.cuh"
 #include "verify.cuh"
+#include "presolve.cuh"
 
 using namespace mc;
 
@@ -221,10 +222,11 @@ void mc_pdlp_default_options(mc_pdlp_options* o) {
 }
 
 int mc_pdlp_struct_sizes(size_t* sizes, int count) {
-    const size_t all[5] = {sizeof(mc_lp), sizeof(mc_pdlp_options), sizeof(mc_pdlp_result), sizeof(mc_pdlp_trace),
-                           sizeof(mc_verify_report)};
+    const size_t all[8] = {sizeof(mc_lp),           sizeof(mc_pdlp_options),    sizeof(mc_pdlp_result),
+                           sizeof(mc_pdlp_trace),   sizeof(mc_verify_report),   sizeof(mc_canonical_lp),
+                           sizeof(mc_presolve_options), sizeof(mc_presolve_info)};
     if (!sizes || count < 0) return set_error(MC_ERR_INVALID_ARGUMENT, "bad sizes buffer");
-    for (int q = 0; q < count && q < 5; ++q) sizes[q] = all[q];
+    for (int q = 0; q < count && q < 8; ++q) sizes[q] = all[q];
     return MC_OK;
 }
 

@@ -73,6 +73,30 @@ Plan make_plan(const Ctx& ctx, int m, int n, long long nnz, int force_col, int f
 // ------------------------------------------------------------- transpose
 // CSR(A) from CSC(A): count, scan, scatter, per-row sort (ascending column,
 // so the layout and every SpMV over it are run-to-run deterministic).
+// In-place inclusive scan of data[0..len), multi-level over tile totals; tmp
+// holds (len + 1) / kScanTile + 4096 ints.
+void inclusive_scan(Ctx& ctx, int* data, long long len, int* tmp, int kind = MC_KERNEL_SETUP) {
+    cudaStream_t s = ctx.stream;
+    std::vector<std::pair<int*, long long>> levels;
+    while (true) {
+        const long long tiles = (len + kScanTile - 1) / kScanTile;
+        ctx.begin_launch(kind);
+        k_scan_tiles<<<(unsigned)tiles, kScanThreads, 0, s>>>(data, len, tmp);
+        ctx.end_launch();
+        levels.push_back({data, len});
+        if (tiles == 1) break;
+        data = tmp;
+        len = tiles;
+        tmp += (tiles + 255) & ~255LL;
+    }
+    for (int l = (int)levels.size() - 2; l >= 0; --l) {
+        const long long tiles = (levels[l].second + kScanTile - 1) / kScanTile;
+        ctx.begin_launch(kind);
+        k_scan_add<<<(unsigned)tiles, kBlock, 0, s>>>(levels[l].first, levels[l].second, levels[l + 1].first);
+        ctx.end_launch();
+    }
+}
+
 int build_csr(Ctx& ctx, int m, int n, long long nnz, const int* csc_start, const int* csc_row,
               const double* csc_val, int* csr_start, int* csr_col, double* csr_val, int* cursor,
               int* long_rows, int* counters /*[2]*/, int* scan_tmp) {
@@ -85,30 +109,7 @@ int build_csr(Ctx& ctx, int m, int n, long long nnz, const int* csc_start, const
         k_count_rows<<<blocks_for(ctx, nnz, kBlock) * 4, kBlock, 0, s>>>(nnz, csc_row, csr_start);
         ctx.end_launch();
     }
-    // inclusive scan of the m+1 counts, multi-level over tile totals
-    std::vector<std::pair<int*, long long>> levels;
-    {
-        int* data = csr_start;
-        long long len = m + 1;
-        int* tmp = scan_tmp;
-        while (true) {
-            const long long tiles = (len + kScanTile - 1) / kScanTile;
-            ctx.begin_launch(MC_KERNEL_SETUP);
-            k_scan_tiles<<<(unsigned)tiles, kScanThreads, 0, s>>>(data, len, tmp);
-            ctx.end_launch();
-            levels.push_back({data, len});
-            if (tiles == 1) break;
-            data = tmp;
-            len = tiles;
-            tmp += (tiles + 255) & ~255LL;
-        }
-        for (int l = (int)levels.size() - 2; l >= 0; --l) {
-            const long long tiles = (levels[l].second + kScanTile - 1) / kScanTile;
-            ctx.begin_launch(MC_KERNEL_SETUP);
-            k_scan_add<<<(unsigned)tiles, kBlock, 0, s>>>(levels[l].first, levels[l].second, levels[l + 1].first);
-            ctx.end_launch();
-        }
-    }
+    inclusive_scan(ctx, csr_start, m + 1, scan_tmp);  // the m+1 counts
     if (nnz == 0) return ctx.launch_check("build_csr");
     const int nb_n = (int)((n + kBlock - 1) / kBlock);
     const int nb_m = (int)((m + kBlock - 1) / kBlock);

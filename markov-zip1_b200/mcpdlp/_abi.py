@@ -154,6 +154,55 @@ class McVerifyReport(C.Structure):
     ]
 
 
+class McCanonicalLp(C.Structure):
+    """mc_canonical_lp: SparseCanonicalModel as plain arrays."""
+    _fields_ = [
+        ("num_rows", C.c_int32),
+        ("num_cols", C.c_int32),
+        ("nnz", C.c_int64),
+        ("col_start", C.c_void_p),
+        ("row_index", C.c_void_p),
+        ("value", C.c_void_p),
+        ("rhs", C.c_void_p),
+        ("objective", C.c_void_p),
+        ("objective_offset", C.c_double),
+    ]
+
+
+class McPresolveOptions(C.Structure):
+    _fields_ = [
+        ("max_passes", C.c_int64),
+        ("feasibility_tolerance", C.c_double),
+        ("dual_tolerance", C.c_double),
+        ("pivot_tolerance", C.c_double),
+    ]
+
+
+class McPresolveInfo(C.Structure):
+    _fields_ = [
+        ("status", C.c_int32),
+        ("message", C.c_char * 96),
+        ("passes_executed", C.c_int64),
+        ("empty_rows_removed", C.c_int64),
+        ("empty_cols_removed", C.c_int64),
+        ("fixed_vars_removed", C.c_int64),
+        ("row_singletons_removed", C.c_int64),
+        ("original_rows", C.c_int64),
+        ("original_cols", C.c_int64),
+        ("presolved_rows", C.c_int64),
+        ("presolved_cols", C.c_int64),
+        ("presolved_nnz", C.c_int64),
+        ("objective_offset", C.c_double),
+        ("records", C.c_int64),
+        ("incident_entries", C.c_int64),
+        ("scan_rounds", C.c_int64),
+        ("presolve_ms", C.c_double),
+    ]
+
+
+MC_RECORD_EMPTY_ROW, MC_RECORD_EMPTY_COLUMN, MC_RECORD_FIXED_VARIABLE, MC_RECORD_ROW_SINGLETON = 0, 1, 2, 3
+
+
 def default_options_struct() -> McPdlpOptions:
     """Defaults of PdlpOptions (include/markov_cero/lp/first_order/pdlp.hpp:18-41)
     plus the engine extensions; identical to mc_pdlp_default_options()."""

@@ -80,6 +80,14 @@ ENGINE_SIGNATURES = {
                          C.c_int),
     "mc_ruiz_equilibrate_noalloc": ([_I32, _I32, _I64, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP,
                                      _VP, _VP, _VP, _I64, _VP, _VP, _VP, _VP], C.c_int),
+    "mc_presolve_default_options": ([_VP], None),
+    "mc_presolve_run": ([_VP, _VP, _VP, _VP], C.c_int),
+    "mc_presolve_get_info": ([_VP, _VP], C.c_int),
+    "mc_presolve_get_model": ([_VP, _VP, _VP, _VP, _VP, _VP], C.c_int),
+    "mc_presolve_get_maps": ([_VP, _VP, _VP], C.c_int),
+    "mc_presolve_get_records": ([_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP], C.c_int),
+    "mc_postsolve": ([_VP, _VP, _VP, _I64, _VP, _I64, _VP, _VP, _VP], C.c_int),
+    "mc_presolve_free": ([_VP], None),
 }
 
 

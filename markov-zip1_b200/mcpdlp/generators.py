@@ -134,3 +134,111 @@ def batch_part2(seed: int, variants: int = 512, m: int = 5000, n: int = 15000, k
 
 def uniform_int(seed: int, index: int, lo: int, hi: int) -> int:
     return int(_lib.lpgen().lpgen_uniform_int(seed, index, lo, hi))
+
+
+def presolve_lp(seed: int, m: int, n: int, k: int = 3, singletons: float = 0.05, chains: int = 4,
+                chain_len: int = 6, empty_rows: float = 0.01, empty_cols: float = 0.01, tiny: float = 0.01,
+                kind: str = "feasible"):
+    """A canonical model (min c.x, A x = rhs, x >= 0) shaped to exercise
+    presolve: about k entries per column; a `singletons` share of rows cut to
+    one entry; `chains` staircases of `chain_len` rows (row t holds the
+    columns of steps t-1 and t) in increasing row order, so that each
+    singleton makes the next row one, and as many in decreasing row order
+    (one step per pass); empty rows and columns; a `tiny` share of entries at
+    1e-13 (below the default pivot tolerance).  rhs = A x* for x* >= 0, so the
+    singletons fix non-negative values.  kind = "infeasible_row" adds an empty
+    row with rhs 1; "infeasible_singleton" a singleton row fixing -1;
+    "unbounded" an empty column with cost -1.  Returns a CanonicalModel."""
+    from .presolve import CanonicalModel
+    rng = np.random.default_rng(seed)
+    rows_of = [set(rng.choice(m, size=min(k, m), replace=False).tolist()) for _ in range(n)]
+    # empty columns
+    for j in rng.choice(n, size=int(empty_cols * n), replace=False):
+        rows_of[j] = set()
+    # staircases: forward (increasing rows) and backward (decreasing rows)
+    used_cols = set()
+    for c in range(2 * chains):
+        rows = np.sort(rng.choice(m, size=chain_len, replace=False))
+        if c % 2:
+            rows = rows[::-1]
+        cols = [j for j in rng.permutation(n)[:4 * chain_len] if j not in used_cols][:chain_len]
+        if len(cols) < chain_len:
+            continue
+        used_cols.update(cols)
+        for j in cols:
+            rows_of[j].difference_update(rows.tolist())
+        for t, r in enumerate(rows):
+            # row r keeps only cols[t] (and cols[t-1]) among all columns
+            for j in range(n):
+                if r in rows_of[j] and j != cols[t] and (t == 0 or j != cols[t - 1]):
+                    rows_of[j].discard(r)
+            rows_of[cols[t]].add(int(r))
+            if t > 0:
+                rows_of[cols[t - 1]].add(int(r))
+    # singleton rows: keep one random entry of the row
+    entries = {}
+    for j in range(n):
+        for r in rows_of[j]:
+            entries.setdefault(r, []).append(j)
+    for r in rng.choice(m, size=int(singletons * m), replace=False):
+        cols = entries.get(int(r), [])
+        if len(cols) > 1:
+            keep = cols[rng.integers(len(cols))]
+            for j in cols:
+                if j != keep:
+                    rows_of[j].discard(int(r))
+    # empty rows
+    for r in rng.choice(m, size=int(empty_rows * m), replace=False):
+        for j in range(n):
+            rows_of[j].discard(int(r))
+    col_start = [0]
+    row_index, value = [], []
+    for j in range(n):
+        for r in sorted(rows_of[j]):
+            v = rng.normal()
+            if v == 0.0:
+                v = 1.0
+            if rng.random() < tiny:
+                v = 1e-13 * (1 if v > 0 else -1)
+            row_index.append(r)
+            value.append(v)
+        col_start.append(len(row_index))
+    col_start = np.array(col_start, np.int32)
+    row_index = np.array(row_index, np.int32)
+    value = np.array(value)
+    x = np.where(rng.random(n) < 0.3, 0.0, rng.uniform(0.5, 3.0, n))
+    rhs = np.zeros(m)
+    for j in range(n):
+        for p in range(col_start[j], col_start[j + 1]):
+            rhs[row_index[p]] += value[p] * x[j]
+    obj = np.abs(rng.normal(size=n)) + 0.1
+    if kind == "infeasible_row":
+        r = int(rng.integers(m))
+        keep = value != 0
+        for j in range(n):
+            for p in range(col_start[j], col_start[j + 1]):
+                if row_index[p] == r:
+                    keep[p] = False
+        col_start = np.concatenate([[0], np.cumsum([keep[col_start[j]:col_start[j + 1]].sum()
+                                                    for j in range(n)])]).astype(np.int32)
+        row_index, value = row_index[keep], value[keep]
+        rhs[r] = 1.0
+    elif kind == "infeasible_singleton":
+        # a new row with a single entry whose value forces x_j = -1
+        j = int(rng.integers(n))
+        m += 1
+        rhs = np.append(rhs, -abs(value[col_start[j]]) if col_start[j + 1] > col_start[j] else -1.0)
+        ins = col_start[j + 1]
+        row_index = np.insert(row_index, ins, m - 1)
+        value = np.insert(value, ins, 1.0)
+        col_start[j + 1:] += 1
+        rhs[-1] = -1.0
+    elif kind == "unbounded":
+        j = int(rng.integers(n))
+        keep = np.ones(len(value), bool)
+        keep[col_start[j]:col_start[j + 1]] = False
+        col_start = np.concatenate([[0], np.cumsum([keep[col_start[q]:col_start[q + 1]].sum()
+                                                    for q in range(n)])]).astype(np.int32)
+        row_index, value = row_index[keep], value[keep]
+        obj[j] = -1.0
+    return CanonicalModel(m, n, col_start, row_index, value, rhs, obj, float(rng.normal()))

@@ -27,6 +27,8 @@ sys.path.insert(0, str(ROOT / "markov-zip1_b200"))
 
 from mcpdlp import _abi  # noqa: E402
 from mcpdlp.model import Model  # noqa: E402
+from mcpdlp.presolve import (CanonicalModel, PostsolveResult, PresolveOptions, PresolveResult,  # noqa: E402
+                             PresolveStack, PresolveStatistics, SolveStatus)
 
 ORACLE_LIB = HERE / "build" / "liboracle_pdlp.so"
 REF_LIB = HERE / "_ref" / "libref_pdlp.so"
@@ -97,6 +99,51 @@ def trace_dict(t, arrays) -> dict:
     return {k: a[: t.count].copy() for k, a in arrays.items()}
 
 
+class _PresolveArrays:
+    """Worst-case output arrays of a presolve of `model` (see presolve_oracle.h)."""
+
+    def __init__(self, model: CanonicalModel):
+        m, n, z = model.num_rows, model.num_cols, model.nnz
+        r = m + n
+        self.cs = np.zeros(n + 1, np.int32)
+        self.ri = np.zeros(max(z, 1), np.int32)
+        self.v = np.zeros(max(z, 1))
+        self.rhs = np.zeros(max(m, 1))
+        self.obj = np.zeros(max(n, 1))
+        self.rmap = np.zeros(max(m, 1), np.int64)
+        self.cmap = np.zeros(max(n, 1), np.int64)
+        self.kind = np.zeros(max(r, 1), np.int32)
+        self.index = np.zeros(max(r, 1), np.int64)
+        self.var = np.zeros(max(r, 1), np.int64)
+        self.val = np.zeros(max(r, 1))
+        self.val2 = np.zeros(max(r, 1))
+        self.ist = np.zeros(r + 1, np.int64)
+        self.irow = np.zeros(max(z, 1), np.int64)
+        self.icoef = np.zeros(max(z, 1))
+
+    def pointers(self) -> list:
+        return [_ptr(a) for a in (self.cs, self.ri, self.v, self.rhs, self.obj, self.rmap, self.cmap, self.kind,
+                                  self.index, self.var, self.val, self.val2, self.ist, self.irow, self.icoef)]
+
+    def result(self, info: _abi.McPresolveInfo) -> PresolveResult:
+        nm, nn, nz = int(info.presolved_rows), int(info.presolved_cols), int(info.presolved_nnz)
+        nr, ni = int(info.records), int(info.incident_entries)
+        st = PresolveStatistics(*(int(getattr(info, f)) for f in (
+            "passes_executed", "empty_rows_removed", "empty_cols_removed", "fixed_vars_removed",
+            "row_singletons_removed", "original_rows", "original_cols", "presolved_rows", "presolved_cols")))
+        cs = self.cs[:nn + 1].copy()
+        if nn == 0:
+            cs = np.zeros(1, np.int32)
+        model = CanonicalModel(nm, nn, cs, self.ri[:nz].copy(), self.v[:nz].copy(), self.rhs[:nm].copy(),
+                               self.obj[:nn].copy(), float(info.objective_offset))
+        stack = PresolveStack(self.kind[:nr].copy(), self.index[:nr].copy(), self.var[:nr].copy(),
+                              self.val[:nr].copy(), self.val2[:nr].copy(), self.ist[:nr + 1].copy(),
+                              self.irow[:ni].copy(), self.icoef[:ni].copy(), self.rmap[:nm].copy(),
+                              self.cmap[:nn].copy())
+        return PresolveResult(SolveStatus(info.status), model, stack, st, info.message.decode(),
+                              dict(presolved_nnz=nz, incident_entries=ni))
+
+
 class OraclePort:
     def __init__(self) -> None:
         if not ORACLE_LIB.exists():
@@ -111,6 +158,11 @@ class OraclePort:
         lib.oracle_spmv.restype = None
         lib.oracle_spmv_t.argtypes = [C.c_int32, C.c_int32] + [_VP] * 5
         lib.oracle_spmv_t.restype = None
+        lib.oracle_presolve.argtypes = [_VP, _VP, _VP, _VP]
+        lib.oracle_presolve.restype = C.c_int
+        lib.oracle_postsolve.argtypes = [_VP, C.c_int64] + [_VP] * 5 + [C.c_int64, _VP, C.c_int64, _VP, _VP,
+                                                                       C.c_int64, _VP, C.c_int64, _VP, _VP, _VP]
+        lib.oracle_postsolve.restype = C.c_int
         self.lib = lib
 
     def solve(self, model: Model, options: _abi.McPdlpOptions, warm_x=None, warm_y=None,
@@ -158,6 +210,37 @@ class OraclePort:
                                _ptr(model.row_index), _ptr(model.value), _ptr(y), _ptr(z))
         return z
 
+    def presolve(self, model: CanonicalModel, options: PresolveOptions | None = None) -> PresolveResult:
+        """The restated presolve (presolve_oracle.c); ValueError where the
+        reference's validate() throws."""
+        o = (options or PresolveOptions()).to_struct()
+        s = model.to_struct()
+        arr = _PresolveArrays(model)
+        out = (C.c_void_p * 15)(*arr.pointers())
+        info = _abi.McPresolveInfo()
+        rc = self.lib.oracle_presolve(C.addressof(s), C.addressof(o), C.addressof(info), C.addressof(out))
+        if rc == _abi.MC_ERR_INVALID_ARGUMENT:
+            raise ValueError("oracle_presolve: invalid canonical model")
+        if rc != 0:
+            raise RuntimeError(f"oracle_presolve failed ({rc})")
+        return arr.result(info)
+
+    def postsolve(self, res: PresolveResult, model: CanonicalModel, primal: np.ndarray,
+                  dual: np.ndarray) -> PostsolveResult:
+        st = res.stack
+        rx = np.ascontiguousarray(primal, dtype=np.float64)
+        ry = np.ascontiguousarray(dual, dtype=np.float64)
+        x, y, obj = np.zeros(model.num_cols), np.zeros(model.num_rows), C.c_double()
+        s = model.to_struct()
+        rc = self.lib.oracle_postsolve(C.addressof(s), st.size(), _ptr(st.kind), _ptr(st.index), _ptr(st.variable),
+                                       _ptr(st.value), _ptr(st.value2), len(st.presolved_to_original_rows),
+                                       _ptr(st.presolved_to_original_rows), len(st.presolved_to_original_cols),
+                                       _ptr(st.presolved_to_original_cols), _ptr(rx), len(rx), _ptr(ry), len(ry),
+                                       _ptr(x), _ptr(y), C.addressof(obj))
+        if rc != 0:
+            raise ValueError(f"oracle_postsolve failed ({rc})")
+        return PostsolveResult(x, y, obj.value)
+
 
 class ReferencePdlp:
     """The reference's compiled CPU code; ``available()`` is False if not built."""
@@ -190,6 +273,14 @@ class ReferencePdlp:
         lib.ref_canonical_equilibrate.restype = C.c_int
         lib.ref_simplex_solve.argtypes = [_VP, C.c_int64, _VP, _VP, _VP, _VP]
         lib.ref_simplex_solve.restype = C.c_int
+        lib.ref_canonical_fetch.argtypes = [_VP] * 6
+        lib.ref_canonical_fetch.restype = C.c_int
+        lib.ref_presolve.argtypes = [_VP, _VP, _VP]
+        lib.ref_presolve.restype = C.c_int
+        lib.ref_presolve_fetch.argtypes = [_VP] * 15
+        lib.ref_presolve_fetch.restype = C.c_int
+        lib.ref_postsolve.argtypes = [_VP, C.c_int64, _VP, C.c_int64, _VP, _VP, _VP]
+        lib.ref_postsolve.restype = C.c_int
         self.lib = lib
 
     def _err(self) -> str:
@@ -322,3 +413,37 @@ class ReferencePdlp:
                                _ptr(rl), _ptr(ru))
         return Model(M, N, cs, ri, v, obj, vl, vu, rl, ru, off.value, s.value,
                      name=Path(path).stem)
+
+    def canonical_model(self, model: Model) -> CanonicalModel:
+        """The CLI's canonical model of `model` (sparse_canonicalize,
+        src/transform/sparse_canonicalize.cpp), unscaled."""
+        lp = model.to_struct()
+        m, n, z = C.c_int64(), C.c_int64(), C.c_int64()
+        if self.lib.ref_canonical_sizes(C.addressof(lp), C.addressof(m), C.addressof(n), C.addressof(z)) != 0:
+            raise RuntimeError(f"reference sparse_canonicalize threw: {self._err()}")
+        m, n, z = m.value, n.value, z.value
+        cs, ri, v = np.zeros(n + 1, np.int32), np.zeros(max(z, 1), np.int32), np.zeros(max(z, 1))
+        rhs, obj, off = np.zeros(max(m, 1)), np.zeros(max(n, 1)), C.c_double()
+        self.lib.ref_canonical_fetch(_ptr(cs), _ptr(ri), _ptr(v), _ptr(rhs), _ptr(obj), C.addressof(off))
+        return CanonicalModel(m, n, cs, ri[:z], v[:z], rhs[:m], obj[:n], off.value)
+
+    def presolve(self, model: CanonicalModel, options: PresolveOptions | None = None) -> PresolveResult:
+        """The reference's presolve (src/presolve/presolve.cpp:20); keeps its
+        result for postsolve().  ValueError where it throws."""
+        o = (options or PresolveOptions()).to_struct()
+        s = model.to_struct()
+        info = _abi.McPresolveInfo()
+        if self.lib.ref_presolve(C.addressof(s), C.addressof(o), C.addressof(info)) != 0:
+            raise ValueError(f"reference presolve threw: {self._err()}")
+        arr = _PresolveArrays(model)
+        self.lib.ref_presolve_fetch(*arr.pointers())
+        return arr.result(info)
+
+    def postsolve(self, model: CanonicalModel, primal: np.ndarray, dual: np.ndarray) -> PostsolveResult:
+        """postsolve() of the last presolve() against its input model."""
+        rx = np.ascontiguousarray(primal, dtype=np.float64)
+        ry = np.ascontiguousarray(dual, dtype=np.float64)
+        x, y, obj = np.zeros(max(model.num_cols, 1)), np.zeros(max(model.num_rows, 1)), C.c_double()
+        if self.lib.ref_postsolve(_ptr(rx), len(rx), _ptr(ry), len(ry), _ptr(x), _ptr(y), C.addressof(obj)) != 0:
+            raise ValueError(f"reference postsolve threw: {self._err()}")
+        return PostsolveResult(x[:model.num_cols], y[:model.num_rows], obj.value)

@@ -9,6 +9,7 @@
 //   verify::verify_primal            src/verify/primal_verifier.cpp:44
 //   lp::reference::solve (simplex)   src/lp/reference/revised_simplex.cpp (small LPs only)
 //   io::parse_mps                    src/io/mps.cpp:96 (fixture generation)
+//   presolve::presolve / postsolve   src/presolve/presolve.cpp:20, :219
 // Only tests, the golden-fixture script and bench.py's reference arm use it.
 #include "mc_pdlp.h"
 
@@ -16,6 +17,7 @@
 #include "markov_cero/lp/first_order/pdlp.hpp"
 #include "markov_cero/lp/reference/revised_simplex.hpp"
 #include "markov_cero/model/model.hpp"
+#include "markov_cero/presolve/presolve.hpp"
 #include "markov_cero/scale/ruiz_scaling.hpp"
 #include "markov_cero/transform/sparse_canonical_model.hpp"
 #include "markov_cero/verify/primal_verifier.hpp"
@@ -26,6 +28,7 @@
 #include <exception>
 #include <fstream>
 #include <string>
+#include <variant>
 #include <vector>
 
 namespace mdl = markov_cero::model;
@@ -366,6 +369,151 @@ int ref_mps_fetch(int32_t* col_start, int32_t* row_index, double* value, double*
         row_upper[i] = from_bound(M.row_upper[i], INFINITY);
     }
     return 0;
+}
+
+// The canonical model kept by ref_canonical_sizes, unscaled.
+int ref_canonical_fetch(int32_t* col_start, int32_t* row_index, double* value, double* rhs, double* obj,
+                        double* offset) {
+    const auto& c = g_canonical;
+    for (std::size_t j = 0; j <= c.matrix.columns; ++j) col_start[j] = (int32_t)c.matrix.column_offsets[j];
+    for (std::size_t p = 0; p < c.matrix.values.size(); ++p) {
+        row_index[p] = (int32_t)c.matrix.row_indices[p];
+        value[p] = c.matrix.values[p];
+    }
+    std::memcpy(rhs, c.rhs.data(), c.matrix.rows * sizeof(double));
+    std::memcpy(obj, c.objective.data(), c.matrix.columns * sizeof(double));
+    *offset = c.objective_offset;
+    return 0;
+}
+
+// presolve() on a canonical model given as arrays (its canonicalisation
+// record is the default one: objective sign +1, no structural-variable map);
+// the result stays here for ref_presolve_fetch and ref_postsolve.
+thread_local markov_cero::transform::SparseCanonicalModel g_pre_in;
+thread_local markov_cero::presolve::PresolveResult g_pre;
+
+int ref_presolve(const mc_canonical_lp* lp, const mc_presolve_options* o, mc_presolve_info* info) {
+    namespace ps = markov_cero::presolve;
+    try {
+        auto& c = g_pre_in;
+        c = markov_cero::transform::SparseCanonicalModel{};
+        c.matrix.rows = (std::size_t)lp->num_rows;
+        c.matrix.columns = (std::size_t)lp->num_cols;
+        c.matrix.column_offsets.assign(lp->col_start, lp->col_start + lp->num_cols + 1);
+        c.matrix.row_indices.assign(lp->row_index, lp->row_index + lp->nnz);
+        c.matrix.values.assign(lp->value, lp->value + lp->nnz);
+        c.rhs.assign(lp->rhs, lp->rhs + lp->num_rows);
+        c.objective.assign(lp->objective, lp->objective + lp->num_cols);
+        c.objective_offset = lp->objective_offset;
+        c.record.objective_sign = 1.0;
+        ps::PresolveOptions po;
+        po.max_passes = (std::size_t)o->max_passes;
+        po.feasibility_tolerance = o->feasibility_tolerance;
+        po.dual_tolerance = o->dual_tolerance;
+        po.pivot_tolerance = o->pivot_tolerance;
+        g_pre = ps::presolve(c, po);
+        std::memset(info, 0, sizeof *info);
+        info->status = (int32_t)g_pre.status;
+        std::snprintf(info->message, sizeof info->message, "%s", g_pre.message.c_str());
+        const auto& st = g_pre.statistics;
+        info->passes_executed = (int64_t)st.passes_executed;
+        info->empty_rows_removed = (int64_t)st.empty_rows_removed;
+        info->empty_cols_removed = (int64_t)st.empty_cols_removed;
+        info->fixed_vars_removed = (int64_t)st.fixed_vars_removed;
+        info->row_singletons_removed = (int64_t)st.row_singletons_removed;
+        info->original_rows = (int64_t)st.original_rows;
+        info->original_cols = (int64_t)st.original_cols;
+        info->presolved_rows = (int64_t)st.presolved_rows;
+        info->presolved_cols = (int64_t)st.presolved_cols;
+        info->presolved_nnz = (int64_t)g_pre.model.matrix.values.size();
+        info->objective_offset = g_pre.model.objective_offset;
+        info->records = (int64_t)g_pre.stack.size();
+        int64_t inc = 0;
+        for (const auto& r : g_pre.stack.records())
+            if (const auto* f = std::get_if<ps::FixedVariableRecord>(&r)) inc += (int64_t)f->row_indices.size();
+        info->incident_entries = inc;
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return 1;
+    }
+}
+
+// The kept presolve result into arrays laid out as mc_presolve_get_model /
+// _get_maps / _get_records give them.
+int ref_presolve_fetch(int32_t* col_start, int32_t* row_index, double* values, double* rhs, double* objective,
+                       int64_t* row_map, int64_t* col_map, int32_t* kind, int64_t* index, int64_t* variable,
+                       double* value, double* value2, int64_t* incident_start, int64_t* incident_row,
+                       double* incident_coefficient) {
+    namespace ps = markov_cero::presolve;
+    const auto& M = g_pre.model;
+    const std::size_t nn = M.matrix.columns;
+    if (M.matrix.column_offsets.size() == nn + 1)
+        for (std::size_t j = 0; j <= nn; ++j) col_start[j] = (int32_t)M.matrix.column_offsets[j];
+    else
+        col_start[0] = 0;
+    for (std::size_t p = 0; p < M.matrix.values.size(); ++p) {
+        row_index[p] = (int32_t)M.matrix.row_indices[p];
+        values[p] = M.matrix.values[p];
+    }
+    for (std::size_t i = 0; i < M.rhs.size(); ++i) rhs[i] = M.rhs[i];
+    for (std::size_t j = 0; j < M.objective.size(); ++j) objective[j] = M.objective[j];
+    const auto& rm = g_pre.stack.presolved_to_original_rows();
+    const auto& cm = g_pre.stack.presolved_to_original_cols();
+    for (std::size_t i = 0; i < rm.size(); ++i) row_map[i] = (int64_t)rm[i];
+    for (std::size_t j = 0; j < cm.size(); ++j) col_map[j] = (int64_t)cm[j];
+    int64_t t = 0, q = 0;
+    incident_start[0] = 0;
+    for (const auto& r : g_pre.stack.records()) {
+        variable[t] = -1;
+        value2[t] = 0.0;
+        if (const auto* e = std::get_if<ps::EmptyRowRecord>(&r)) {
+            kind[t] = MC_RECORD_EMPTY_ROW;
+            index[t] = (int64_t)e->original_row_index;
+            value[t] = e->rhs_value;
+        } else if (const auto* c = std::get_if<ps::EmptyColumnRecord>(&r)) {
+            kind[t] = MC_RECORD_EMPTY_COLUMN;
+            index[t] = (int64_t)c->original_col_index;
+            value[t] = c->objective_coeff;
+            value2[t] = c->fixed_value;
+        } else if (const auto* f = std::get_if<ps::FixedVariableRecord>(&r)) {
+            kind[t] = MC_RECORD_FIXED_VARIABLE;
+            index[t] = (int64_t)f->original_col_index;
+            value[t] = f->fixed_value;
+            value2[t] = f->objective_coeff;
+            for (std::size_t k = 0; k < f->row_indices.size(); ++k, ++q) {
+                incident_row[q] = (int64_t)f->row_indices[k];
+                incident_coefficient[q] = f->coefficients[k];
+            }
+        } else if (const auto* s = std::get_if<ps::RowSingletonRecord>(&r)) {
+            kind[t] = MC_RECORD_ROW_SINGLETON;
+            index[t] = (int64_t)s->original_row_index;
+            variable[t] = (int64_t)s->variable_index;
+            value[t] = s->coefficient;
+            value2[t] = s->rhs_value;
+        }
+        incident_start[++t] = q;
+    }
+    return 0;
+}
+
+// postsolve() of the kept result against the kept input model.
+int ref_postsolve(const double* reduced_primal, int64_t reduced_cols, const double* reduced_dual,
+                  int64_t reduced_rows, double* primal, double* dual, double* objective) {
+    try {
+        markov_cero::lp::reference::Result red;
+        red.status = markov_cero::lp::reference::SolveStatus::optimal;
+        red.primal.assign(reduced_primal, reduced_primal + reduced_cols);
+        red.dual.assign(reduced_dual, reduced_dual + reduced_rows);
+        const auto out = markov_cero::presolve::postsolve(g_pre.stack, red, g_pre_in);
+        std::memcpy(primal, out.primal.data(), out.primal.size() * sizeof(double));
+        std::memcpy(dual, out.dual.data(), out.dual.size() * sizeof(double));
+        *objective = out.objective;
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return 1;
+    }
 }
 
 } // extern "C"

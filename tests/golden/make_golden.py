@@ -24,6 +24,17 @@ Writes, next to this script:
     python tests/golden/make_golden.py --only simplex   # refresh that section
     python tests/golden/make_golden.py --only netlib    # the published Netlib optima
     python tests/golden/make_golden.py --only scale     # larger seeded LPs (minutes)
+    python tests/golden/make_golden.py --only presolve  # presolve / postsolve of canonical models
+
+The ``presolve`` section holds the reference's presolve and postsolve
+(src/presolve/presolve.cpp) on canonical models: the models of the
+reference's presolve unit tests (tests/presolve_test.cpp:30-96, written out
+as canon_*.npz), the canonical form (sparse_canonicalize) of the Netlib
+fixtures, and seeded generated models (mcpdlp.generators.presolve_lp, pinned
+by a SHA-256 of the generated arrays) in all four outcomes; per model the
+status, message, statistics, objective offset and SHA-256 digests of the
+reduced model, the record stack and the maps, and of postsolve's primal and
+dual for a seeded reduced solution.
 
 The ``scale`` section holds the reference solve_pdlp on seeded LPs far above
 the unit-test sizes: the 40M-nonzero LP's generator at m = 200,000,
@@ -180,6 +191,88 @@ def scale_section() -> dict:
     return out
 
 
+PRESOLVE_GENERATED = [  # (name, seed, m, n, kind)
+    ("gen_feasible_s1", 1, 200, 300, "feasible"),
+    ("gen_feasible_s2", 2, 400, 500, "feasible"),
+    ("gen_feasible_s3", 3, 120, 150, "feasible"),
+    ("gen_infeasible_row_s4", 4, 200, 300, "infeasible_row"),
+    ("gen_infeasible_singleton_s5", 5, 200, 300, "infeasible_singleton"),
+    ("gen_unbounded_s6", 6, 200, 300, "unbounded"),
+]
+
+
+def presolve_unit_models() -> list:
+    """The canonical models of the reference's presolve tests
+    (tests/presolve_test.cpp:30-96); the blend LP there goes through
+    sparse_canonicalize as in the test."""
+    from mcpdlp.presolve import CanonicalModel
+    out = [
+        ("canon_empty_row", CanonicalModel(1, 1, [0, 0], [], [], [10.0], [1.0])),
+        ("canon_empty_column", CanonicalModel(1, 1, [0, 0], [], [], [0.0], [-5.0])),
+        ("canon_row_singleton", CanonicalModel(2, 2, [0, 2, 3], [0, 1, 1], [2.0, 1.0, 1.0], [6.0, 7.0],
+                                               [10.0, 5.0])),
+    ]
+    return out
+
+
+def presolve_blend_lp() -> Model:
+    # tests/presolve_test.cpp:12-28: min 40 A + 30 B, A + B = 100, 0.01 A + 0.03 B <= 2, A, B >= 0
+    inf = np.inf
+    return from_triplets(2, 2, [0, 0, 1, 1], [0, 1, 0, 1], [1.0, 1.0, 0.01, 0.03], objective=[40.0, 30.0],
+                         var_lower=[0.0, 0.0], var_upper=[inf, inf], row_lower=[100.0, -inf],
+                         row_upper=[100.0, 2.0], name="presolve_blend")
+
+
+def save_canonical(c, name: str) -> None:
+    np.savez_compressed(HERE / f"{name}.npz", num_rows=c.num_rows, num_cols=c.num_cols, col_start=c.col_start,
+                        row_index=c.row_index, value=c.value, rhs=c.rhs, objective=c.objective,
+                        objective_offset=c.objective_offset)
+
+
+def canonical_digest(c) -> str:
+    return sha(np.array([c.num_rows, c.num_cols]), c.col_start, c.row_index, c.value, c.rhs, c.objective,
+               np.array([c.objective_offset]))
+
+
+def presolve_record(ref, c) -> dict:
+    import dataclasses
+    try:
+        r = ref.presolve(c)
+    except ValueError as e:
+        return dict(error=str(e))
+    st = r.stack
+    out = dict(status=int(r.status), message=r.message, statistics=dataclasses.asdict(r.statistics),
+               objective_offset=r.model.objective_offset, model_sha256=canonical_digest(r.model),
+               stack_sha256=sha(st.kind, st.index, st.variable, st.value, st.value2, st.incident_start,
+                                st.incident_row, st.incident_coefficient),
+               maps_sha256=sha(st.presolved_to_original_rows, st.presolved_to_original_cols))
+    if r.status == 0:
+        rng = np.random.default_rng(7)
+        rx = rng.uniform(0.0, 2.0, r.model.num_cols)
+        ry = rng.normal(size=r.model.num_rows)
+        p = ref.postsolve(c, rx, ry)
+        out["post"] = dict(seed=7, primal_sha256=sha(p.primal), dual_sha256=sha(p.dual), objective=p.objective)
+    return out
+
+
+def presolve_section(ref) -> dict:
+    out = {}
+    cases = presolve_unit_models()
+    cases.append(("canon_presolve_blend", ref.canonical_model(presolve_blend_lp())))
+    for name in NETLIB:
+        cases.append((f"canon_netlib_{name}", ref.canonical_model(ref.parse_mps(REF / "data/netlib" / f"{name}.mps"))))
+    for name, c in cases:
+        save_canonical(c, name)
+        out[name] = dict(file=f"{name}.npz", digest=canonical_digest(c), m=c.num_rows, n=c.num_cols, nnz=c.nnz,
+                         result=presolve_record(ref, c))
+        print(name, out[name]["result"].get("status"), out[name]["result"].get("statistics"))
+    for name, seed, m_, n_, kind in PRESOLVE_GENERATED:
+        c = generators.presolve_lp(seed, m_, n_, kind=kind)
+        out[name] = dict(seed=seed, m=m_, n=n_, kind=kind, digest=canonical_digest(c), result=presolve_record(ref, c))
+        print(name, out[name]["result"].get("status"), out[name]["result"].get("message"))
+    return out
+
+
 def main() -> None:
     orc.build(reference=True)
     ref = orc.ReferencePdlp()
@@ -192,6 +285,8 @@ def main() -> None:
             golden["netlib_optimal"] = netlib_optima()
         elif what == "scale":
             golden["scale"] = scale_section()
+        elif what == "presolve":
+            golden["presolve"] = presolve_section(ref)
         (HERE / "golden.json").write_text(json.dumps(golden, indent=1, sort_keys=True))
         return
     golden = {"models": {}, "synthetic": {}, "ruiz": {}}
@@ -223,6 +318,7 @@ def main() -> None:
     golden["simplex"] = simplex_section(ref)
     golden["netlib_optimal"] = netlib_optima()
     golden["scale"] = scale_section()
+    golden["presolve"] = presolve_section(ref)
     (HERE / "golden.json").write_text(json.dumps(golden, indent=1, sort_keys=True))
 
 

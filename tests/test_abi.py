@@ -53,11 +53,12 @@ def test_library_loads_with_signatures():
 
 
 def test_struct_layouts_match():
-    sizes = (C.c_size_t * 5)()
-    assert _lib.engine().mc_pdlp_struct_sizes(sizes, 5) == 0
+    sizes = (C.c_size_t * 8)()
+    assert _lib.engine().mc_pdlp_struct_sizes(sizes, 8) == 0
     assert list(sizes) == [C.sizeof(_abi.McLp), C.sizeof(_abi.McPdlpOptions),
                            C.sizeof(_abi.McPdlpResult), C.sizeof(_abi.McPdlpTrace),
-                           C.sizeof(_abi.McVerifyReport)]
+                           C.sizeof(_abi.McVerifyReport), C.sizeof(_abi.McCanonicalLp),
+                           C.sizeof(_abi.McPresolveOptions), C.sizeof(_abi.McPresolveInfo)]
 
 
 def test_default_options_match_reference_defaults():
