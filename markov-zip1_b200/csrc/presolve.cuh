@@ -19,14 +19,17 @@
 //   decided).  A round counts every row >= P; a row with one entry is a
 //   tentative singleton, and among those with the same column only the first
 //   fires (atomicMin per column; the later ones find the column fixed and
-//   have no entry left).  The first row r >= P with two or more entries that
-//   a tentative singleton below it would reduce is the boundary B: every
-//   tentative singleton below B fires exactly as in the sequential walk (no
-//   earlier singleton of the round touches its row), nothing at or above B is
-//   decided yet.  The round commits the singletons below B, applies their
-//   substitutions, and moves P to B.  Each round commits at least one
-//   singleton or ends the walk, so rounds <= singletons + 1 (one round when
-//   no singleton feeds another).
+//   have no entry left).  A row r with c >= 2 entries of which h are fixed by
+//   tentative singletons below it has c - h entries left at its turn; the
+//   first such row with c - h = 1 is the boundary B (a singleton the round
+//   did not foresee).  Every tentative singleton below B fires exactly as in
+//   the sequential walk and no other row below B does (induction over the
+//   rows: the singletons below a row are the tentative ones, so its count at
+//   its turn is c - h), nothing at or above B is decided yet.  The round
+//   commits the singletons below B, applies their substitutions, and moves P
+//   to B.  Each round commits at least one singleton or ends the walk, so
+//   rounds <= singletons + 1, and one round suffices when no singleton makes
+//   another.
 // * Substitutions: every row applies the fixes of the round that touch it in
 //   the order of their singleton rows -- the order of the walk -- with the
 //   same operands (rhs -= a * fixed, rounded separately), so the right-hand
@@ -180,21 +183,22 @@ __global__ void kp_close_step(int which, int len, const int* __restrict__ scan, 
 __global__ void kp_single_scan(int m, const int* __restrict__ rs, const int* __restrict__ ci,
                                const double* __restrict__ rv, const unsigned char* __restrict__ col_act,
                                const unsigned char* __restrict__ row_act, double tol, int* __restrict__ cnt,
-                               int* __restrict__ sc, double* __restrict__ sa, int* __restrict__ col_first,
-                               const PsCtl* __restrict__ ctl) {
+                               int* __restrict__ hits, int* __restrict__ sc, double* __restrict__ sa,
+                               int* __restrict__ col_first, const PsCtl* __restrict__ ctl) {
     if (ctl->stop) return;
     const int P = ctl->P;
     for (int i = P + blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
         int c = 0, j = -1;
         double a = 0.0;
         if (row_act[i])
-            for (int p = rs[i]; p < rs[i + 1] && c < 2; ++p)
+            for (int p = rs[i]; p < rs[i + 1]; ++p)
                 if (col_act[ci[p]] && fabs(rv[p]) > tol) {
                     ++c;
                     j = ci[p];
                     a = rv[p];
                 }
         cnt[i] = c;
+        hits[i] = 0;
         if (c == 1) {
             sc[i] = j;
             sa[i] = a;
@@ -203,13 +207,15 @@ __global__ void kp_single_scan(int m, const int* __restrict__ rs, const int* __r
     }
 }
 
-// Tentative singletons (first bidder of their column); the boundary; the
-// first singleton whose value would be negative.
+// Tentative singletons (first bidder of their column); for every later row
+// with two or more entries, how many of them the tentative singletons fix;
+// the first singleton whose value would be negative.
 __global__ void kp_tentative(int m, const int* __restrict__ cs, const int* __restrict__ ri,
                              const double* __restrict__ v, const unsigned char* __restrict__ row_act,
-                             const int* __restrict__ cnt, const int* __restrict__ sc, const double* __restrict__ sa,
-                             const int* __restrict__ col_first, const double* __restrict__ rhs, double tol,
-                             double feas, unsigned char* __restrict__ fire, PsCtl* __restrict__ ctl) {
+                             const int* __restrict__ cnt, int* __restrict__ hits, const int* __restrict__ sc,
+                             const double* __restrict__ sa, const int* __restrict__ col_first,
+                             const double* __restrict__ rhs, double tol, double feas, unsigned char* __restrict__ fire,
+                             PsCtl* __restrict__ ctl) {
     if (ctl->stop) return;
     const int P = ctl->P;
     for (int i = P + blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
@@ -220,9 +226,19 @@ __global__ void kp_tentative(int m, const int* __restrict__ cs, const int* __res
         const int j = sc[i];
         for (int p = cs[j]; p < cs[j + 1]; ++p) {
             const int r = ri[p];
-            if (r > i && row_act[r] && cnt[r] >= 2 && fabs(v[p]) > tol) atomicMin(&ctl->boundary, r);
+            if (r > i && row_act[r] && cnt[r] >= 2 && fabs(v[p]) > tol) atomicAdd(&hits[r], 1);
         }
     }
+}
+
+// the boundary: the first row >= P left with exactly one entry by the
+// tentative singletons below it
+__global__ void kp_boundary(int m, const unsigned char* __restrict__ row_act, const int* __restrict__ cnt,
+                            const int* __restrict__ hits, PsCtl* __restrict__ ctl) {
+    if (ctl->stop) return;
+    const int P = ctl->P;
+    for (int r = P + blockIdx.x * blockDim.x + threadIdx.x; r < m; r += gridDim.x * blockDim.x)
+        if (hits[r] > 0 && row_act[r] && cnt[r] >= 2 && cnt[r] - hits[r] == 1) atomicMin(&ctl->boundary, r);
 }
 
 // limit of this round; flag[i] = singleton committed this round
@@ -299,12 +315,13 @@ __global__ void kp_incident_count(int len, const int* __restrict__ cs, const int
     }
 }
 
+// the incident lists of the round's singletons; marks the rows they touch
 __global__ void kp_incident_fill(const int* __restrict__ cs, const int* __restrict__ ri, const double* __restrict__ v,
                                  const unsigned char* __restrict__ row_act, double tol,
                                  const int* __restrict__ fire_col, const int* __restrict__ inc_scan, PsRecords R,
-                                 const PsCtl* __restrict__ ctl) {
+                                 int* __restrict__ touched, const PsCtl* __restrict__ ctl) {
     if (ctl->stop) return;
-    const int nf = ctl->nfires;
+    const int nf = ctl->nfires, round = ctl->round;
     const long long base = ctl->rec, ibase = ctl->inc;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nf; q += gridDim.x * blockDim.x) {
         const int j = fire_col[q];
@@ -314,6 +331,7 @@ __global__ void kp_incident_fill(const int* __restrict__ cs, const int* __restri
             if (row_act[ri[p]] && fabs(v[p]) > tol) {
                 R.inc_row[w] = ri[p];
                 R.inc_coef[w] = v[p];
+                touched[ri[p]] = round;
                 ++w;
             }
         const long long t = base + 2LL * q + 1;
@@ -322,17 +340,17 @@ __global__ void kp_incident_fill(const int* __restrict__ cs, const int* __restri
     }
 }
 
-// Each active row applies this round's fixes of its columns in the order of
+// Each row the round's singletons touch applies their fixes in the order of
 // their singleton rows: rhs -= a * fixed (presolve.cpp:155-159).
 __global__ void kp_substitute(int m, const int* __restrict__ rs, const int* __restrict__ ci,
-                              const double* __restrict__ rv, const unsigned char* __restrict__ row_act, double tol,
+                              const double* __restrict__ rv, const int* __restrict__ touched, double tol,
                               const int* __restrict__ fix_round, const int* __restrict__ fix_row,
                               const double* __restrict__ fix_val, double* __restrict__ rhs,
                               const PsCtl* __restrict__ ctl) {
     if (ctl->stop || ctl->nfires == 0) return;
     const int round = ctl->round;
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < m; r += gridDim.x * blockDim.x) {
-        if (!row_act[r]) continue;
+        if (touched[r] != round) continue;
         const int b = rs[r], e = rs[r + 1];
         int k = 0;
         for (int p = b; p < e; ++p) k += fix_round[ci[p]] == round && fabs(rv[p]) > tol;
@@ -663,8 +681,8 @@ int presolve_body(Ctx& ctx, const mc_canonical_lp* lp, const mc_presolve_options
     }
     PsScratch S(s);
     const size_t lines = (size_t)std::max(m, n) + 1;
-    int *rs, *ci, *cursor, *long_rows, *counters, *scan_tmp, *cnt, *sc, *col_first, *flag, *fix_round, *fix_row,
-        *fire_col, *inc_cnt, *new_row, *cc;
+    int *rs, *ci, *cursor, *long_rows, *counters, *scan_tmp, *cnt, *hits, *sc, *col_first, *flag, *fix_round,
+        *fix_row, *fire_col, *inc_cnt, *new_row, *cc, *touched;
     double *rv, *rhs, *sa, *fix_val;
     unsigned char *row_act, *col_act, *fire;
     PsCtl* ctl;
@@ -682,6 +700,8 @@ int presolve_body(Ctx& ctx, const mc_canonical_lp* lp, const mc_presolve_options
     S.get(&col_act, nn);
     S.get(&fire, mm);
     S.get(&cnt, mm);
+    S.get(&hits, mm);
+    S.get(&touched, mm);
     S.get(&sc, mm);
     S.get(&col_first, nn);
     S.get(&flag, lines);
@@ -734,11 +754,56 @@ int presolve_body(Ctx& ctx, const mc_canonical_lp* lp, const mc_presolve_options
     CU(cudaMemsetAsync(col_act, 1, nn, s));
     CU(cudaMemsetAsync(col_first, 0x7f, sizeof(int) * nn, s));  // above every row index
     CU(cudaMemsetAsync(fix_round, 0xff, sizeof(int) * nn, s));  // -1
+    CU(cudaMemsetAsync(touched, 0xff, sizeof(int) * mm, s));
     CU(cudaMemsetAsync(cnt, 0, sizeof(int) * mm, s));
     CU(cudaMemsetAsync(ctl, 0, sizeof(PsCtl), s));
     const double tol = o->pivot_tolerance;
     const int gm = blocks_for(ctx, std::max(m, 1), kBlock), gn = blocks_for(ctx, std::max(n, 1), kBlock);
     const PsRecords R = P->R;
+    // One round of the singleton walk (all its sizes are fixed and its scan
+    // position lives on the device), captured once as a graph and replayed.
+    auto enqueue_round = [&]() {
+        kp_single_scan<<<gm, kBlock, 0, s>>>(m, rs, ci, rv, col_act, row_act, tol, cnt, hits, sc, sa, col_first,
+                                             ctl);
+        kp_tentative<<<gm, kBlock, 0, s>>>(m, P->cs, P->ri, P->v, row_act, cnt, hits, sc, sa, col_first, rhs, tol,
+                                           o->feasibility_tolerance, fire, ctl);
+        kp_boundary<<<gm, kBlock, 0, s>>>(m, row_act, cnt, hits, ctl);
+        kp_round_limit<<<1, 1, 0, s>>>(m, ctl);
+        kp_fire_flags<<<gm, kBlock, 0, s>>>(m, fire, flag, ctl);
+        inclusive_scan(ctx, flag, m, scan_tmp, MC_KERNEL_OTHER);
+        kp_commit<<<gm, kBlock, 0, s>>>(m, flag, sc, sa, rhs, P->obj, row_act, col_act, fix_round, fix_row, fix_val,
+                                        fire_col, R, ctl);
+        kp_fire_count<<<1, 1, 0, s>>>(m, flag, ctl);
+        kp_incident_count<<<gm, kBlock, 0, s>>>(m, P->cs, P->ri, P->v, row_act, tol, fire_col, inc_cnt, ctl);
+        inclusive_scan(ctx, inc_cnt, m, scan_tmp, MC_KERNEL_OTHER);
+        kp_incident_fill<<<gm, kBlock, 0, s>>>(P->cs, P->ri, P->v, row_act, tol, fire_col, inc_cnt, R, touched, ctl);
+        kp_substitute<<<gm, kBlock, 0, s>>>(m, rs, ci, rv, touched, tol, fix_round, fix_row, fix_val, rhs, ctl);
+        kp_clear_bids<<<gm, kBlock, 0, s>>>(m, cnt, sc, col_first, ctl);
+        kp_close_round<<<1, 1, 0, s>>>(m, inc_cnt, ctl);
+    };
+    cudaGraphExec_t round_graph = nullptr;
+    struct GraphGuard {
+        cudaGraphExec_t* g;
+        ~GraphGuard() {
+            if (*g) cudaGraphExecDestroy(*g);
+        }
+    } graph_guard{&round_graph};
+    auto capture_round = [&]() -> int {
+        CU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        ctx.capturing = true;
+        enqueue_round();
+        ctx.capturing = false;
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(s, &g);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture", __LINE__);
+        const cudaError_t e2 = cudaGraphInstantiate(&round_graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e2 != cudaSuccess) {
+            round_graph = nullptr;
+            return cuda_fail(e2, "cudaGraphInstantiate", __LINE__);
+        }
+        return MC_OK;
+    };
     PsCtl h{};
     long long pass = 0, rounds = 0;
     for (; pass < o->max_passes; ++pass) {
@@ -762,25 +827,8 @@ int presolve_body(Ctx& ctx, const mc_canonical_lp* lp, const mc_presolve_options
         // 3. row singletons (presolve.cpp:119-167), in rounds
         while (true) {
             if (m > 0) {
-                kp_single_scan<<<gm, kBlock, 0, s>>>(m, rs, ci, rv, col_act, row_act, tol, cnt, sc, sa, col_first,
-                                                     ctl);
-                kp_tentative<<<gm, kBlock, 0, s>>>(m, P->cs, P->ri, P->v, row_act, cnt, sc, sa, col_first, rhs, tol,
-                                                   o->feasibility_tolerance, fire, ctl);
-                kp_round_limit<<<1, 1, 0, s>>>(m, ctl);
-                kp_fire_flags<<<gm, kBlock, 0, s>>>(m, fire, flag, ctl);
-                inclusive_scan(ctx, flag, m, scan_tmp, MC_KERNEL_OTHER);
-                kp_commit<<<gm, kBlock, 0, s>>>(m, flag, sc, sa, rhs, P->obj, row_act, col_act, fix_round, fix_row,
-                                                fix_val, fire_col, R, ctl);
-                kp_fire_count<<<1, 1, 0, s>>>(m, flag, ctl);
-                kp_incident_count<<<gm, kBlock, 0, s>>>(m, P->cs, P->ri, P->v, row_act, tol, fire_col, inc_cnt,
-                                                        ctl);
-                inclusive_scan(ctx, inc_cnt, m, scan_tmp, MC_KERNEL_OTHER);
-                kp_incident_fill<<<gm, kBlock, 0, s>>>(P->cs, P->ri, P->v, row_act, tol, fire_col, inc_cnt, R,
-                                                       ctl);
-                kp_substitute<<<gm, kBlock, 0, s>>>(m, rs, ci, rv, row_act, tol, fix_round, fix_row, fix_val, rhs,
-                                                    ctl);
-                kp_clear_bids<<<gm, kBlock, 0, s>>>(m, cnt, sc, col_first, ctl);
-                kp_close_round<<<1, 1, 0, s>>>(m, inc_cnt, ctl);
+                if (!round_graph) TRY(capture_round());
+                CU(cudaGraphLaunch(round_graph, s));
                 ++rounds;
             }
             CU(cudaMemcpyAsync(&h, ctl, sizeof h, cudaMemcpyDeviceToHost, s));

@@ -242,3 +242,53 @@ def presolve_lp(seed: int, m: int, n: int, k: int = 3, singletons: float = 0.05,
         row_index, value = row_index[keep], value[keep]
         obj[j] = -1.0
     return CanonicalModel(m, n, col_start, row_index, value, rhs, obj, float(rng.normal()))
+
+
+def presolve_workload(seed: int, m: int, n: int, k: int = 4, singletons: float = 0.05, chains: int = 64,
+                      chain_len: int = 32, empty_rows: float = 0.01, empty_cols: float = 0.01,
+                      tiny: float = 0.001):
+    """A large canonical model for timing presolve, built with numpy only
+    (presolve_lp's shape at scale): about k entries per column, a
+    `singletons` share of rows cut to one entry, `chains` staircases of
+    `chain_len` rows (half in increasing row order: one pass each; half
+    decreasing: one step per pass), empty rows and columns, a `tiny` share of
+    entries at 1e-13.  rhs = A x* for x* >= 0.  Returns a CanonicalModel."""
+    from .presolve import CanonicalModel
+    rng = np.random.default_rng(seed)
+    cols = np.repeat(np.arange(n, dtype=np.int64), k)
+    rows = rng.integers(0, m, size=n * k, dtype=np.int64)
+    key = np.unique(cols * m + rows)  # distinct (column, row) pairs, column-major
+    cols, rows = key // m, key % m
+    drop = np.zeros(len(rows), bool)
+    drop |= np.isin(rows, rng.choice(m, size=int(empty_rows * m), replace=False))
+    drop |= np.isin(cols, rng.choice(n, size=int(empty_cols * n), replace=False))
+    # staircases on fresh rows and columns
+    c_rows = rng.choice(m, size=chains * chain_len, replace=False).reshape(chains, chain_len)
+    c_rows.sort(axis=1)
+    c_rows[1::2] = c_rows[1::2, ::-1]
+    c_cols = rng.choice(n, size=chains * chain_len, replace=False).reshape(chains, chain_len)
+    drop |= np.isin(rows, c_rows.ravel()) | np.isin(cols, c_cols.ravel())
+    # singleton rows: one entry kept (the one with the smallest random key)
+    s_rows = rng.choice(m, size=int(singletons * m), replace=False)
+    in_s = np.isin(rows, s_rows) & ~drop
+    idx = np.nonzero(in_s)[0]
+    order = idx[np.lexsort((rng.random(len(idx)), rows[idx]))]
+    first = np.ones(len(order), bool)
+    first[1:] = rows[order[1:]] != rows[order[:-1]]
+    drop[order[~first]] = True
+    rows, cols = rows[~drop], cols[~drop]
+    add_r = np.concatenate([c_rows.ravel(), c_rows[:, 1:].ravel()])
+    add_c = np.concatenate([c_cols.ravel(), c_cols[:, :-1].ravel()])
+    key = np.unique(np.concatenate([cols * m + rows, add_c * m + add_r]))
+    cols, rows = key // m, key % m
+    value = rng.normal(size=len(rows))
+    value[value == 0.0] = 1.0
+    t = rng.random(len(rows)) < tiny
+    value[t] = np.copysign(1e-13, value[t])
+    col_start = np.zeros(n + 1, np.int64)
+    np.add.at(col_start, cols + 1, 1)
+    col_start = np.cumsum(col_start).astype(np.int32)
+    x = np.where(rng.random(n) < 0.3, 0.0, rng.uniform(0.5, 3.0, n))
+    rhs = np.bincount(rows, weights=value * x[cols], minlength=m).astype(np.float64)
+    obj = np.abs(rng.normal(size=n)) + 0.1
+    return CanonicalModel(m, n, col_start, rows.astype(np.int32), value, rhs, obj, float(rng.normal()))

@@ -447,3 +447,24 @@ class ReferencePdlp:
         if self.lib.ref_postsolve(_ptr(rx), len(rx), _ptr(ry), len(ry), _ptr(x), _ptr(y), C.addressof(obj)) != 0:
             raise ValueError(f"reference postsolve threw: {self._err()}")
         return PostsolveResult(x[:model.num_cols], y[:model.num_rows], obj.value)
+
+
+def presolve_mismatch(a: PresolveResult, b: PresolveResult) -> str | None:
+    """The first field in which two presolve results differ (bit for bit),
+    or None if they are identical."""
+    if a.status != b.status or a.message != b.message:
+        return f"status/message {a.status}:{a.message!r} vs {b.status}:{b.message!r}"
+    if a.statistics != b.statistics:
+        return f"statistics {a.statistics} vs {b.statistics}"
+    if (a.model.num_rows, a.model.num_cols) != (b.model.num_rows, b.model.num_cols):
+        return "reduced model shape"
+    if a.model.objective_offset != b.model.objective_offset:
+        return f"objective offset {a.model.objective_offset!r} vs {b.model.objective_offset!r}"
+    for f in ("col_start", "row_index", "value", "rhs", "objective"):
+        if not np.array_equal(getattr(a.model, f), getattr(b.model, f)):
+            return f"reduced model {f}"
+    for f in ("kind", "index", "variable", "value", "value2", "incident_start", "incident_row",
+              "incident_coefficient", "presolved_to_original_rows", "presolved_to_original_cols"):
+        if not np.array_equal(getattr(a.stack, f), getattr(b.stack, f)):
+            return f"stack {f}"
+    return None
