@@ -611,6 +611,16 @@ int mc_presolve_get_records(const mc_presolve* p, int32_t* kind, int64_t* index,
 int mc_postsolve(mc_pdlp_ctx* ctx, const mc_presolve* p, const double* reduced_primal, int64_t reduced_cols,
                  const double* reduced_dual, int64_t reduced_rows, double* primal, double* dual, double* objective);
 void mc_presolve_free(mc_presolve* p);
+/* A presolve result rebuilt from a stack held by the caller (for a caller
+ * that keeps the reference's PresolveStack, presolve_stack.hpp:41-72, and
+ * wants mc_postsolve on it): `original` is the model presolve ran on, the
+ * record arrays are as mc_presolve_get_records gives them (incident lists are
+ * not needed by postsolve), the maps as mc_presolve_get_maps.  Host arrays.
+ * Indices out of range or unknown kinds are MC_ERR_INVALID_ARGUMENT. */
+int mc_presolve_load(mc_pdlp_ctx* ctx, const mc_canonical_lp* original, int64_t records, const int32_t* kind,
+                     const int64_t* index, const int64_t* variable, const double* value, const double* value2,
+                     int64_t presolved_rows, const int64_t* row_map, int64_t presolved_cols, const int64_t* col_map,
+                     mc_presolve** out);
 
 #ifdef __cplusplus
 }

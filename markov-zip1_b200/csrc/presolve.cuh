@@ -941,6 +941,118 @@ int presolve_run(Ctx& ctx, const mc_canonical_lp* lp, const mc_presolve_options*
     return MC_OK;
 }
 
+int presolve_load(Ctx& ctx, const mc_canonical_lp* lp, long long nrec, const int* kind, const long long* index,
+                  const long long* variable, const double* value, const double* value2, long long pm,
+                  const long long* row_map, long long pn, const long long* col_map, mc_presolve** out) {
+    if (!out) return set_error(MC_ERR_INVALID_ARGUMENT, "presolve load: null result pointer");
+    *out = nullptr;
+    if (!lp || nrec < 0 || pm < 0 || pn < 0 || (nrec > 0 && (!kind || !index || !variable || !value || !value2)) ||
+        (pm > 0 && !row_map) || (pn > 0 && !col_map))
+        return set_error(MC_ERR_INVALID_ARGUMENT, "presolve load: null argument");
+    const int m = lp->num_rows, n = lp->num_cols;
+    if (m < 0 || n < 0 || lp->nnz < 0 || !lp->col_start || (n > 0 && !lp->objective) ||
+        (lp->nnz > 0 && (!lp->row_index || !lp->value)))
+        return set_error(MC_ERR_INVALID_ARGUMENT, "presolve load: malformed canonical model");
+    if (nrec > (long long)m + n || pm > m || pn > n)
+        return set_error(MC_ERR_INVALID_ARGUMENT, "presolve load: more records or map entries than lines");
+    // the records and maps index the model's lines (postsolve reads through them)
+    for (long long t = 0; t < nrec; ++t) {
+        const long long i = index[t];
+        switch (kind[t]) {
+            case MC_RECORD_EMPTY_ROW:
+                if (i < 0 || i >= m) return set_error(MC_ERR_INVALID_ARGUMENT, "record %lld: row out of range", t);
+                break;
+            case MC_RECORD_EMPTY_COLUMN:
+            case MC_RECORD_FIXED_VARIABLE:
+                if (i < 0 || i >= n) return set_error(MC_ERR_INVALID_ARGUMENT, "record %lld: column out of range", t);
+                break;
+            case MC_RECORD_ROW_SINGLETON:
+                if (i < 0 || i >= m || variable[t] < 0 || variable[t] >= n || value[t] == 0.0)
+                    return set_error(MC_ERR_INVALID_ARGUMENT, "record %lld: bad row singleton", t);
+                break;
+            default: return set_error(MC_ERR_INVALID_ARGUMENT, "record %lld: unknown kind %d", t, kind[t]);
+        }
+    }
+    for (long long q = 0; q < pm; ++q)
+        if (row_map[q] < 0 || row_map[q] >= m) return set_error(MC_ERR_INVALID_ARGUMENT, "row map out of range");
+    for (long long q = 0; q < pn; ++q)
+        if (col_map[q] < 0 || col_map[q] >= n) return set_error(MC_ERR_INVALID_ARGUMENT, "column map out of range");
+    ctx.drop_session();
+    cudaStream_t s = ctx.stream;
+    mc_presolve* P = new mc_presolve();
+    P->device = ctx.device;
+    P->m = m;
+    P->n = n;
+    P->nnz = lp->nnz;
+    P->offset = lp->objective_offset;
+    const size_t nn = (size_t)n + 1, zz = (size_t)lp->nnz + 1, rr = (size_t)nrec + 1;
+    int rc = MC_OK;
+    auto own = [&](auto** ptr, size_t count) {
+        if (rc == MC_OK) rc = ps_alloc(P, reinterpret_cast<void**>(ptr), count * sizeof(**ptr));
+    };
+    own(&P->cs, nn);
+    own(&P->ri, zz);
+    own(&P->v, zz);
+    own(&P->obj, nn);
+    own(&P->row_map, (size_t)pm + 1);
+    own(&P->col_map, (size_t)pn + 1);
+    own(&P->R.kind, rr);
+    own(&P->R.index, rr);
+    own(&P->R.variable, rr);
+    own(&P->R.value, rr);
+    own(&P->R.value2, rr);
+    own(&P->R.inc_off, rr);
+    own(&P->R.inc_len, rr);
+    if (rc == MC_OK) {
+        rc = [&]() -> int {
+            const cudaMemcpyKind k = cudaMemcpyDefault;
+            CU(cudaMemcpyAsync(P->cs, lp->col_start, sizeof(int) * nn, k, s));
+            if (lp->nnz > 0) {
+                CU(cudaMemcpyAsync(P->ri, lp->row_index, sizeof(int) * lp->nnz, k, s));
+                CU(cudaMemcpyAsync(P->v, lp->value, sizeof(double) * lp->nnz, k, s));
+            }
+            if (n > 0) CU(cudaMemcpyAsync(P->obj, lp->objective, sizeof(double) * n, k, s));
+            if (pm > 0) CU(cudaMemcpyAsync(P->row_map, row_map, sizeof(long long) * pm, k, s));
+            if (pn > 0) CU(cudaMemcpyAsync(P->col_map, col_map, sizeof(long long) * pn, k, s));
+            if (nrec > 0) {
+                CU(cudaMemcpyAsync(P->R.kind, kind, sizeof(int) * nrec, k, s));
+                CU(cudaMemcpyAsync(P->R.index, index, sizeof(long long) * nrec, k, s));
+                CU(cudaMemcpyAsync(P->R.variable, variable, sizeof(long long) * nrec, k, s));
+                CU(cudaMemcpyAsync(P->R.value, value, sizeof(double) * nrec, k, s));
+                CU(cudaMemcpyAsync(P->R.value2, value2, sizeof(double) * nrec, k, s));
+                CU(cudaMemsetAsync(P->R.inc_len, 0, sizeof(int) * nrec, s));
+            }
+            CU(cudaStreamSynchronize(s));
+            // the column structure postsolve walks (singleton columns), checked like presolve's input
+            int* bad = nullptr;
+            CU(cudaMallocAsync(reinterpret_cast<void**>(&bad), sizeof(int), s));
+            CU(cudaMemsetAsync(bad, 0, sizeof(int), s));
+            if (n > 0) k_validate_csc<<<(n + kBlock - 1) / kBlock, kBlock, 0, s>>>(m, n, lp->nnz, P->cs, P->ri, P->v, bad);
+            int hb = 0;
+            CU(cudaMemcpyAsync(&hb, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+            CU(cudaFreeAsync(bad, s));
+            CU(cudaStreamSynchronize(s));
+            TRY(ctx.launch_check("presolve load"));
+            if (hb) return set_error(MC_ERR_INVALID_ARGUMENT, "presolve load: invalid canonical CSC (flags %d)", hb);
+            return MC_OK;
+        }();
+    }
+    if (rc != MC_OK) {
+        ps_free(P);
+        return rc;
+    }
+    mc_presolve_info& I = P->info;
+    I.status = MC_PRESOLVE_OPTIMAL;
+    I.original_rows = m;
+    I.original_cols = n;
+    I.presolved_rows = pm;
+    I.presolved_cols = pn;
+    I.records = nrec;
+    std::snprintf(I.message, sizeof I.message, "loaded");
+    *out = P;
+    return MC_OK;
+}
+
 int postsolve_body(Ctx& ctx, const mc_presolve* P, const double* rx, long long rx_len, const double* ry,
                    long long ry_len, double* x_out, double* y_out, double* objective) {
     cudaStream_t s = ctx.stream;
@@ -1135,3 +1247,18 @@ extern "C" int mc_postsolve(mc_pdlp_ctx* c, const mc_presolve* p, const double* 
 }
 
 extern "C" void mc_presolve_free(mc_presolve* p) { mc::ps_free(p); }
+
+extern "C" int mc_presolve_load(mc_pdlp_ctx* c, const mc_canonical_lp* original, int64_t records,
+                                const int32_t* kind, const int64_t* index, const int64_t* variable,
+                                const double* value, const double* value2, int64_t presolved_rows,
+                                const int64_t* row_map, int64_t presolved_cols, const int64_t* col_map,
+                                mc_presolve** out) {
+    using namespace mc;
+    Ctx* ctx = reinterpret_cast<Ctx*>(c);
+    if (!ctx) return set_error(MC_ERR_INVALID_ARGUMENT, "context is NULL");
+    DeviceGuard guard(ctx->device);
+    return presolve_load(*ctx, original, records, kind, reinterpret_cast<const long long*>(index),
+                         reinterpret_cast<const long long*>(variable), value, value2, presolved_rows,
+                         reinterpret_cast<const long long*>(row_map), presolved_cols,
+                         reinterpret_cast<const long long*>(col_map), out);
+}

@@ -88,6 +88,7 @@ ENGINE_SIGNATURES = {
     "mc_presolve_get_records": ([_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP], C.c_int),
     "mc_postsolve": ([_VP, _VP, _VP, _I64, _VP, _I64, _VP, _VP, _VP], C.c_int),
     "mc_presolve_free": ([_VP], None),
+    "mc_presolve_load": ([_VP, _VP, _I64, _VP, _VP, _VP, _VP, _VP, _I64, _VP, _I64, _VP, _VP], C.c_int),
 }
 
 

@@ -1,18 +1,22 @@
-"""Node-LP relaxations of branch and bound, solved as one GPU batch.
+"""Node-LP relaxations of branch and bound, solved together on the GPU.
 
 The reference solves each open node's LP relaxation on its own with the dense
 simplex (``solve_node_relaxation``, src/milp/node_lp.cpp:9-82, capped at 1024
-canonical rows).  Here all the nodes of one branching round go to the engine's
-batched PDLP (``mc_pdlp_ctx_solve_batch``) together: every node is the parent
-model with tightened variable bounds (src/milp/milp_solver.cpp:401-447), so a
-round is exactly the batch of node variants the batched engine is built for.
+canonical rows).  Here all the nodes of one branching round go to the engine
+together.  Every node is the parent model with tightened variable bounds
+(src/milp/milp_solver.cpp:401-447), so when the nodes share the matrix, the
+objective and the row bounds -- the normal case -- they run in the variant
+engine (``mc_pdlp_ctx_solve_variants``: the matrix stored and read once per
+iteration for all of them); nodes of different models run in the packed batch
+(``mc_pdlp_ctx_solve_batch``).
 
     results = solve_node_relaxations(ctx, [down, up, ...], max_iterations=100000)
 
-Statuses are the reference's ``lp::reference::SolveStatus`` names.  A node
-whose bounds cross, or whose row activity interval misses a row's bounds, is
-certified ``infeasible`` at setup (the engine's certificates); PDLP does not
-otherwise detect infeasibility, so such a node ends at ``iteration_limit``.
+Statuses are the reference's ``lp::reference::SolveStatus`` names.  A node is
+``infeasible`` when the engine certifies it: crossed bounds or a row activity
+interval that misses a row's bounds (at setup), or a dual ray found during the
+iterations (Farkas certificate); an infeasible node that yields no certificate
+ends at ``iteration_limit``.
 """
 from __future__ import annotations
 
@@ -31,7 +35,7 @@ SOLVE_STATUS = ("optimal", "infeasible", "unbounded", "iteration_limit", "invali
 
 _FROM_PDLP = {
     PdlpStatus.optimal: "optimal",
-    PdlpStatus.infeasible_or_unbounded: "infeasible",   # certified at setup
+    PdlpStatus.infeasible_or_unbounded: "infeasible",   # certified (setup or dual ray)
     PdlpStatus.iteration_limit: "iteration_limit",
     PdlpStatus.numerical_failure: "numerical_failure",
 }
@@ -47,24 +51,52 @@ class NodeLpResult:
     iterations: int = 0
 
 
+def share_matrix(nodes: list) -> bool:
+    """True when every node has the first node's matrix, objective, offset,
+    sense and row bounds (they differ at most in their variable bounds)."""
+    a = nodes[0]
+    same = lambda x, y: x is y or (x.shape == y.shape and np.array_equal(x, y))  # noqa: E731
+    for b in nodes[1:]:
+        if (b.num_rows, b.num_cols, b.nnz, b.objective_offset, int(b.objective_sense)) != \
+                (a.num_rows, a.num_cols, a.nnz, a.objective_offset, int(a.objective_sense)):
+            return False
+        if not all(same(getattr(a, f), getattr(b, f)) for f in ("col_start", "row_index", "value", "objective",
+                                                                 "row_lower", "row_upper")):
+            return False
+    return True
+
+
 def solve_node_relaxations(ctx: Context, nodes: list, max_iterations: int = 500000,
                            feasibility_tolerance: float = 1e-7,
                            precision: Precision = Precision.fp64,
                            options: Optional[PdlpOptions] = None,
-                           warm_primal: Optional[list] = None, warm_dual: Optional[list] = None) -> list:
-    """LP relaxations of `nodes` (Models) in one batched solve.  The defaults
-    are milp::Options' max_iterations and feasibility_tolerance
+                           warm_primal: Optional[list] = None, warm_dual: Optional[list] = None,
+                           shared_matrix: Optional[bool] = None) -> list:
+    """LP relaxations of `nodes` (Models) solved together.  The defaults are
+    milp::Options' max_iterations and feasibility_tolerance
     (include/markov_cero/milp/milp_solver.hpp:15-32); the tolerance is the
     PDLP relative KKT tolerance.  warm_primal / warm_dual (a point or None per
     node) start each node where its parent ended, as the reference's node
     solve starts the dual simplex from the parent's basis
-    (src/milp/node_lp.cpp:44-60)."""
+    (src/milp/node_lp.cpp:44-60).  shared_matrix: None = the variant engine
+    when the nodes share the matrix (share_matrix), True / False to force
+    the variant engine / the packed batch."""
     o = options or PdlpOptions()
     o.max_iterations = max_iterations
     o.set_tolerance(feasibility_tolerance)
     o.precision = precision
+    nodes = list(nodes)
+    if shared_matrix is None:
+        shared_matrix = len(nodes) > 1 and share_matrix(nodes)
+    if shared_matrix:
+        if not share_matrix(nodes):
+            raise ValueError("shared_matrix=True needs nodes that differ only in their variable bounds")
+        res = ctx.solve_variants(nodes[0], [n_.var_lower for n_ in nodes], [n_.var_upper for n_ in nodes], o,
+                                 initial_primal=warm_primal, initial_dual=warm_dual)
+    else:
+        res = ctx.solve_batch(nodes, o, initial_primal=warm_primal, initial_dual=warm_dual)
     out = []
-    for r in ctx.solve_batch(list(nodes), o, initial_primal=warm_primal, initial_dual=warm_dual):
+    for r in res:
         res = NodeLpResult(status=_FROM_PDLP[r.status], iterations=r.iterations)
         if res.status == "optimal":
             res.primal = r.primal

@@ -8,6 +8,9 @@ markov-zip1_b200/binding/_build/:
 * pdlp_test -- the reference's tests/pdlp_test.cpp (asserts on).  With
   MARKOV_CERO_PDLP_BACKEND=gpu every solve_pdlp of the process goes to the
   GPU engine; with no visible GPU that must fail loudly (no CPU fallback).
+* presolve_test -- the reference's tests/presolve_test.cpp with its
+  presolve()/postsolve() calls routed to the device presolve
+  (binding/presolve_gpu.cpp); with no visible GPU it must fail loudly.
 * markov-cero-solve -- the reference CLI with `--engine pdlp-gpu`
   (apps/markov_cero_solve.cpp:136-189), checked on the ADR-P3-05 model
   (docs/decisions/ADR-P3-05-pdhg-pdlp.md:11-23: objective -9.0000013 at
@@ -33,6 +36,7 @@ from test_oracle import GOLDEN, load_model
 BUILD = Path(__file__).resolve().parent.parent / "markov-zip1_b200" / "binding" / "_build"
 PDLP_TEST = BUILD / "pdlp_test"
 CLI = BUILD / "markov-cero-solve"
+PRESOLVE_TEST = BUILD / "presolve_test"
 
 needs_build = pytest.mark.skipif(not (PDLP_TEST.exists() and CLI.exists()),
                                  reason="integration build absent (needs the reference sources)")
@@ -105,6 +109,13 @@ def test_reference_pdlp_test_cpu_backend_through_dispatch():
     assert "All PDLP unit tests PASSED" in r.stdout
 
 
+@pytest.mark.skipif(not PRESOLVE_TEST.exists(), reason="integration build absent (needs the reference sources)")
+def test_reference_presolve_test_without_device_fails_loudly():
+    r = run([PRESOLVE_TEST], {"CUDA_VISIBLE_DEVICES": ""})
+    assert r.returncode != 0
+    assert "no CPU fallback" in (r.stdout + r.stderr)
+
+
 @needs_build
 def test_gpu_request_without_device_fails_loudly():
     # a GPU request never falls back to the CPU solver
@@ -148,6 +159,18 @@ def test_cli_cpu_pdlp_on_written_netlib_matches_golden(tmp_path):
 
 
 # ------------------------------------------------------------------- GPU
+@pytest.mark.skipif(not PRESOLVE_TEST.exists(), reason="integration build absent (needs the reference sources)")
+@pytest.mark.gpu
+def test_reference_presolve_test_on_gpu():
+    """tests/presolve_test.cpp (asserts on): infeasible empty row, unbounded
+    empty column, the row-singleton reduction and its postsolve (x = (3, 4),
+    objective 50), and the blend model with presolve against the simplex
+    without it -- every presolve/postsolve on the device."""
+    r = run([PRESOLVE_TEST])
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "presolve tests passed" in r.stdout
+
+
 @needs_build
 @pytest.mark.gpu
 def test_reference_pdlp_test_on_gpu():

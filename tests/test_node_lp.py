@@ -98,3 +98,40 @@ def test_children_warm_started_from_the_parent(gpu_ctx):
     for c, w in both:
         assert rel(c.objective, w.objective) <= 1e-5
     assert sum(w.iterations for _, w in both) < 0.8 * sum(c.iterations for c, _ in both)
+
+
+@pytest.mark.gpu
+def test_shared_matrix_round_matches_the_packed_batch(gpu_ctx):
+    """A round whose nodes share the matrix runs in the variant engine by
+    default; it must give the packed batch's statuses and objectives."""
+    base = generators.random_lp(23, 300, 900, 6)
+    parent = solve_node_relaxations(gpu_ctx, [base], max_iterations=100000, feasibility_tolerance=1e-7)[0]
+    x = parent.primal
+    order = np.argsort(-np.abs(x - np.round(x)))[:10]
+    nodes = []
+    for j in order:
+        nodes += [c for c in branch_children(base, x, int(j)) if c is not None]
+    nodes += [generators.tighten_bounds(base, 200 + s)[0] for s in range(4)]
+    from mcpdlp.node_lp import share_matrix
+    assert share_matrix(nodes)
+    shared = solve_node_relaxations(gpu_ctx, nodes, max_iterations=100000, feasibility_tolerance=1e-7)
+    packed = solve_node_relaxations(gpu_ctx, nodes, max_iterations=100000, feasibility_tolerance=1e-7,
+                                    shared_matrix=False)
+    for node, a, b in zip(nodes, shared, packed):
+        assert a.status == b.status, node.name
+        if a.status == "optimal":
+            assert rel(a.objective, b.objective) <= 1e-6, node.name
+
+
+def test_share_matrix_detects_other_models():
+    a = generators.random_lp(5, 30, 90, 4)
+    b = a.copy()
+    b.var_upper = b.var_upper.copy()
+    b.var_upper[3] = 1.0
+    from mcpdlp.node_lp import share_matrix
+    assert share_matrix([a, b])
+    c = a.copy()
+    c.objective = c.objective.copy()
+    c.objective[0] += 1.0
+    assert not share_matrix([a, c])
+    assert not share_matrix([a, generators.random_lp(6, 30, 90, 4)])
