@@ -65,6 +65,7 @@ struct PsCtl {
     int nfires;     // singletons committed this round
     int round;      // rounds so far (marks the columns fixed in a round)
     int cause;      // what stopped it: 0 empty row, 1 empty column, 2 negative singleton
+    int full;       // 1 in a pass's first round: count every row; later rounds keep the counts
     long long rec;   // records on the stack
     long long inc;   // incident entries on the stack
     long long reductions;  // this pass
@@ -180,6 +181,9 @@ __global__ void kp_close_step(int which, int len, const int* __restrict__ scan, 
 
 // ------------------------------------------------------------------ step 3
 // Counts of the undecided rows (>= P); one-entry rows bid for their column.
+// The first round of a pass counts every row; later rounds use the counts
+// that the substitutions keep up to date (a count changes only when one of
+// the row's columns is fixed, kp_substitute).
 __global__ void kp_single_scan(int m, const int* __restrict__ rs, const int* __restrict__ ci,
                                const double* __restrict__ rv, const unsigned char* __restrict__ col_act,
                                const unsigned char* __restrict__ row_act, double tol, int* __restrict__ cnt,
@@ -187,7 +191,13 @@ __global__ void kp_single_scan(int m, const int* __restrict__ rs, const int* __r
                                int* __restrict__ col_first, const PsCtl* __restrict__ ctl) {
     if (ctl->stop) return;
     const int P = ctl->P;
+    const bool full = ctl->full;
     for (int i = P + blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        hits[i] = 0;
+        if (!full) {
+            if (row_act[i] && cnt[i] == 1) atomicMin(&col_first[sc[i]], i);
+            continue;
+        }
         int c = 0, j = -1;
         double a = 0.0;
         if (row_act[i])
@@ -198,7 +208,6 @@ __global__ void kp_single_scan(int m, const int* __restrict__ rs, const int* __r
                     a = rv[p];
                 }
         cnt[i] = c;
-        hits[i] = 0;
         if (c == 1) {
             sc[i] = j;
             sa[i] = a;
@@ -241,15 +250,13 @@ __global__ void kp_boundary(int m, const unsigned char* __restrict__ row_act, co
         if (hits[r] > 0 && row_act[r] && cnt[r] >= 2 && cnt[r] - hits[r] == 1) atomicMin(&ctl->boundary, r);
 }
 
-// limit of this round; flag[i] = singleton committed this round
-__global__ void kp_round_limit(int m, PsCtl* __restrict__ ctl) {
-    if (ctl->stop) return;
-    ctl->L = min(min(ctl->boundary, ctl->first_bad), m);
-}
-
+// flag[i] = singleton committed this round: tentative and below this
+// round's limit L = min(boundary, first negative singleton, m)
 __global__ void kp_fire_flags(int m, const unsigned char* __restrict__ fire, int* __restrict__ flag,
-                              const PsCtl* __restrict__ ctl) {
-    const int P = ctl->P, L = ctl->stop ? 0 : ctl->L;
+                              PsCtl* __restrict__ ctl) {
+    const int P = ctl->P;
+    const int L = ctl->stop ? 0 : min(min(ctl->boundary, ctl->first_bad), m);
+    if (blockIdx.x == 0 && threadIdx.x == 0 && !ctl->stop) ctl->L = L;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
         flag[i] = (i >= P && i < L && fire[i]) ? 1 : 0;
 }
@@ -292,19 +299,16 @@ __global__ void kp_commit(int m, const int* __restrict__ scan, const int* __rest
     }
 }
 
-__global__ void kp_fire_count(int m, const int* __restrict__ scan, PsCtl* __restrict__ ctl) {
-    if (ctl->stop) return;
-    const int P = ctl->P, L = ctl->L;
-    ctl->nfires = (L > P) ? scan[L - 1] - (P > 0 ? scan[P - 1] : 0) : 0;
-}
-
 // incident rows of each committed singleton's column (rows active after the
 // commit; 0 past the round's singletons, so that the scan over len is defined)
 __global__ void kp_incident_count(int len, const int* __restrict__ cs, const int* __restrict__ ri, const double* __restrict__ v,
                                   const unsigned char* __restrict__ row_act, double tol,
-                                  const int* __restrict__ fire_col, int* __restrict__ inc_cnt,
-                                  const PsCtl* __restrict__ ctl) {
-    const int nf = ctl->stop ? 0 : ctl->nfires;
+                                  const int* __restrict__ fire_col, const int* __restrict__ fire_scan,
+                                  int* __restrict__ inc_cnt, PsCtl* __restrict__ ctl) {
+    // the round's singletons: the flags below P are 0, so the scan at L-1 counts them
+    const int L = ctl->L;
+    const int nf = (ctl->stop || L <= ctl->P) ? 0 : fire_scan[L - 1];
+    if (blockIdx.x == 0 && threadIdx.x == 0 && !ctl->stop) ctl->nfires = nf;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < len; q += gridDim.x * blockDim.x) {
         int c = 0;
         if (q < nf) {
@@ -341,12 +345,14 @@ __global__ void kp_incident_fill(const int* __restrict__ cs, const int* __restri
 }
 
 // Each row the round's singletons touch applies their fixes in the order of
-// their singleton rows: rhs -= a * fixed (presolve.cpp:155-159).
+// their singleton rows: rhs -= a * fixed (presolve.cpp:155-159), and keeps
+// its count of surviving entries.
 __global__ void kp_substitute(int m, const int* __restrict__ rs, const int* __restrict__ ci,
                               const double* __restrict__ rv, const int* __restrict__ touched, double tol,
                               const int* __restrict__ fix_round, const int* __restrict__ fix_row,
-                              const double* __restrict__ fix_val, double* __restrict__ rhs,
-                              const PsCtl* __restrict__ ctl) {
+                              const double* __restrict__ fix_val, const unsigned char* __restrict__ col_act,
+                              int* __restrict__ cnt, int* __restrict__ sc, double* __restrict__ sa,
+                              double* __restrict__ rhs, const PsCtl* __restrict__ ctl) {
     if (ctl->stop || ctl->nfires == 0) return;
     const int round = ctl->round;
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < m; r += gridDim.x * blockDim.x) {
@@ -357,6 +363,15 @@ __global__ void kp_substitute(int m, const int* __restrict__ rs, const int* __re
         if (k == 0) continue;
         double h = rhs[r];
         int last = -1;
+        // the row loses k entries; left with one, it records that one
+        const int left = cnt[r] - k;
+        cnt[r] = left;
+        if (left == 1)
+            for (int p = b; p < e; ++p)
+                if (col_act[ci[p]] && fabs(rv[p]) > tol) {
+                    sc[r] = ci[p];
+                    sa[r] = rv[p];
+                }
         for (int t = 0; t < k; ++t) {  // k fixes, smallest singleton row first
             int best = kNone;
             double a = 0.0, f = 0.0;
@@ -394,6 +409,7 @@ __global__ void kp_close_round(int m, const int* __restrict__ inc_scan, PsCtl* _
     ctl->stats[2] += nf;
     ctl->stats[3] += nf;
     ctl->round += 1;
+    ctl->full = 0;
     if (ctl->first_bad != kNone && ctl->first_bad == ctl->L) {  // presolve.cpp:137-142
         ctl->stop = 1;
         ctl->cause = 2;
@@ -407,6 +423,7 @@ __global__ void kp_close_round(int m, const int* __restrict__ inc_scan, PsCtl* _
 
 __global__ void kp_begin_pass(PsCtl* __restrict__ ctl) {
     ctl->reductions = 0;
+    ctl->full = 1;
     ctl->first_bad = ctl->first_unb = ctl->boundary = kNone;
     ctl->P = 0;
 }
@@ -768,16 +785,16 @@ int presolve_body(Ctx& ctx, const mc_canonical_lp* lp, const mc_presolve_options
         kp_tentative<<<gm, kBlock, 0, s>>>(m, P->cs, P->ri, P->v, row_act, cnt, hits, sc, sa, col_first, rhs, tol,
                                            o->feasibility_tolerance, fire, ctl);
         kp_boundary<<<gm, kBlock, 0, s>>>(m, row_act, cnt, hits, ctl);
-        kp_round_limit<<<1, 1, 0, s>>>(m, ctl);
         kp_fire_flags<<<gm, kBlock, 0, s>>>(m, fire, flag, ctl);
         inclusive_scan(ctx, flag, m, scan_tmp, MC_KERNEL_OTHER);
         kp_commit<<<gm, kBlock, 0, s>>>(m, flag, sc, sa, rhs, P->obj, row_act, col_act, fix_round, fix_row, fix_val,
                                         fire_col, R, ctl);
-        kp_fire_count<<<1, 1, 0, s>>>(m, flag, ctl);
-        kp_incident_count<<<gm, kBlock, 0, s>>>(m, P->cs, P->ri, P->v, row_act, tol, fire_col, inc_cnt, ctl);
+        kp_incident_count<<<gm, kBlock, 0, s>>>(m, P->cs, P->ri, P->v, row_act, tol, fire_col, flag, inc_cnt,
+                                                ctl);
         inclusive_scan(ctx, inc_cnt, m, scan_tmp, MC_KERNEL_OTHER);
         kp_incident_fill<<<gm, kBlock, 0, s>>>(P->cs, P->ri, P->v, row_act, tol, fire_col, inc_cnt, R, touched, ctl);
-        kp_substitute<<<gm, kBlock, 0, s>>>(m, rs, ci, rv, touched, tol, fix_round, fix_row, fix_val, rhs, ctl);
+        kp_substitute<<<gm, kBlock, 0, s>>>(m, rs, ci, rv, touched, tol, fix_round, fix_row, fix_val, col_act, cnt,
+                                            sc, sa, rhs, ctl);
         kp_clear_bids<<<gm, kBlock, 0, s>>>(m, cnt, sc, col_first, ctl);
         kp_close_round<<<1, 1, 0, s>>>(m, inc_cnt, ctl);
     };

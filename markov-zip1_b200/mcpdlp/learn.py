@@ -162,7 +162,7 @@ def solve_targets(ctx: Context, models: list, options: PdlpOptions, batch: int =
 
 
 def solve_warm(ctx: Context, net: WarmStartNet, model: Model, options: PdlpOptions,
-               guard: bool = True, use_weight: bool = False) -> PdlpResult:
+               guard: bool = True, use_weight: bool = False, halves: str = "both") -> PdlpResult:
     """Solve from the network's prediction, guarded by the engine (guard=False
     forces the prediction, for measuring what it does on its own).
 
@@ -172,10 +172,14 @@ def solve_warm(ctx: Context, net: WarmStartNet, model: Model, options: PdlpOptio
     config-0 family LPs at 1e-8: 844 iterations from the predicted weight
     alone, 869 from the solve's own final weight, 736 cold), while the
     predicted point with the derived weight takes 676.  use_weight=True passes
-    the predicted weight too."""
+    the predicted weight too.  halves: "both", "dual" (the predicted dual with
+    the cold primal start) or "primal"."""
+    if halves not in ("both", "dual", "primal"):
+        raise ValueError("halves must be 'both', 'dual' or 'primal'")
     x, y, lw = net.predict(model)
     o = PdlpOptions(**{k: getattr(options, k) for k in options.__dataclass_fields__})
-    o.initial_primal, o.initial_dual = x, y
+    o.initial_primal = x if halves in ("both", "primal") else None
+    o.initial_dual = y if halves in ("both", "dual") else None
     o.initial_primal_weight = float(min(max(math.exp(lw), 1e-6), 1e6)) if use_weight else 0.0
     o.warm_start_guard = guard
     return ctx.solve(model, o)
