@@ -660,7 +660,7 @@ def run_engine_arm(args) -> None:
         forms["speedup_time_to_1e-8_fp32_refine_vs_fp64"] = (forms["fp64"]["time_to_tol_s"]
                                                             / forms["fp32_refine"]["time_to_tol_s"])
 
-    # ---- the learned warm start (the north star's combined form): a network
+    # ---- the learned warm start (FP32 + refinement + GNN start, combined): a network
     # trained on GPU-solved LPs of the same generator at small sizes (m in
     # [200, 600], n = 3m, 1024 seeds), its dual prediction for this LP fed to
     # the engine with the guard on (the engine keeps the cold start if the

@@ -18,8 +18,9 @@ markov-zip1_b200/binding/_build/:
   published optima.
 
 The MPS files are written here from the committed fixtures (parsed by the
-reference's own reader when they were made), so the GPU box needs no
-reference checkout; the binaries are built where the reference sources are.
+reference's own reader when they were made), so a machine that runs these
+tests needs no reference checkout; the binaries are built where the
+reference sources are.
 """
 from __future__ import annotations
 
