@@ -47,9 +47,12 @@
 #include "verify.cuh"
 
 #include <climits>
+#include <cooperative_groups.h>
 #include <vector>
 
 namespace mc {
+
+namespace cg = cooperative_groups;
 
 constexpr int kNone = INT_MAX;
 
@@ -61,11 +64,8 @@ struct PsCtl {
     int first_unb;  // step 2: first empty column with negative cost
     int boundary;   // step 3: first row a tentative singleton below it reduces
     int P;          // step 3 scan position
-    int L;          // this round's commit limit
-    int nfires;     // singletons committed this round
     int round;      // rounds so far (marks the columns fixed in a round)
     int cause;      // what stopped it: 0 empty row, 1 empty column, 2 negative singleton
-    int full;       // 1 in a pass's first round: count every row; later rounds keep the counts
     long long rec;   // records on the stack
     long long inc;   // incident entries on the stack
     long long reductions;  // this pass
@@ -180,250 +180,284 @@ __global__ void kp_close_step(int which, int len, const int* __restrict__ scan, 
 }
 
 // ------------------------------------------------------------------ step 3
-// Counts of the undecided rows (>= P); one-entry rows bid for their column.
-// The first round of a pass counts every row; later rounds use the counts
-// that the substitutions keep up to date (a count changes only when one of
-// the row's columns is fixed, kp_substitute).
-__global__ void kp_single_scan(int m, const int* __restrict__ rs, const int* __restrict__ ci,
-                               const double* __restrict__ rv, const unsigned char* __restrict__ col_act,
-                               const unsigned char* __restrict__ row_act, double tol, int* __restrict__ cnt,
-                               int* __restrict__ hits, int* __restrict__ sc, double* __restrict__ sa,
-                               int* __restrict__ col_first, const PsCtl* __restrict__ ctl) {
-    if (ctl->stop) return;
-    const int P = ctl->P;
-    const bool full = ctl->full;
-    for (int i = P + blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
-        hits[i] = 0;
-        if (!full) {
-            if (row_act[i] && cnt[i] == 1) atomicMin(&col_first[sc[i]], i);
-            continue;
+// The singleton walk of one pass is one cooperative kernel: each block owns a
+// contiguous range of rows, the phases of a round are separated by grid-wide
+// barriers, and the rounds repeat on the device until the walk ends (at most
+// m + 1 rounds; each round commits a singleton or ends the walk).  Phases:
+//   1 counts of the rows >= P (every row in a pass's first round, later the
+//     counts the substitutions keep) and bids of one-entry rows for their
+//     column (atomicMin: the first bidder is the tentative singleton);
+//   2 tentative singletons; hits on the later rows of their columns; the
+//     first singleton whose value would be negative;
+//   3 the boundary (first row left with one entry by the hits); bids cleared;
+//   4 the limit L = min(boundary, first negative, m); singletons per block;
+//   5 commit below L in row order (block prefix + block scan), incident
+//     counts;
+//   6 incident lists in stack order, touched rows marked;
+//   7 substitutions in the touched rows, counts kept; the round closed.
+struct Walk {
+    int m;
+    const int *rs, *ci;
+    const double* rv;
+    const int *cs, *ri;
+    const double* v;
+    const double* obj;
+    unsigned char *row_act, *col_act, *fire;
+    int *cnt, *hits, *sc, *col_first, *fix_round, *fix_row, *fire_col, *inc_cnt, *touched;
+    double *sa, *fix_val, *rhs;
+    int *block_fires, *block_inc;
+    double tol, feas;
+    PsRecords R;
+    PsCtl* ctl;
+};
+
+constexpr int kWalkThreads = 256;
+constexpr int kWalkWarps = kWalkThreads / 32;
+
+// Exclusive prefix of v over the block's threads in thread order; *total
+// receives the block's sum.  Every thread of the block must call it.
+__device__ __forceinline__ int block_exclusive(int v, int* sh, int* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sh[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int w = lane < kWalkWarps ? sh[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
         }
-        int c = 0, j = -1;
-        double a = 0.0;
-        if (row_act[i])
-            for (int p = rs[i]; p < rs[i + 1]; ++p)
-                if (col_act[ci[p]] && fabs(rv[p]) > tol) {
-                    ++c;
-                    j = ci[p];
-                    a = rv[p];
-                }
-        cnt[i] = c;
-        if (c == 1) {
-            sc[i] = j;
-            sa[i] = a;
-            atomicMin(&col_first[j], i);
-        }
+        if (lane < kWalkWarps) sh[lane] = w;
     }
+    __syncthreads();
+    const int before = (warp > 0 ? sh[warp - 1] : 0) + x - v;
+    *total = sh[kWalkWarps - 1];
+    __syncthreads();
+    return before;
 }
 
-// Tentative singletons (first bidder of their column); for every later row
-// with two or more entries, how many of them the tentative singletons fix;
-// the first singleton whose value would be negative.
-__global__ void kp_tentative(int m, const int* __restrict__ cs, const int* __restrict__ ri,
-                             const double* __restrict__ v, const unsigned char* __restrict__ row_act,
-                             const int* __restrict__ cnt, int* __restrict__ hits, const int* __restrict__ sc,
-                             const double* __restrict__ sa, const int* __restrict__ col_first,
-                             const double* __restrict__ rhs, double tol, double feas, unsigned char* __restrict__ fire,
-                             PsCtl* __restrict__ ctl) {
-    if (ctl->stop) return;
-    const int P = ctl->P;
-    for (int i = P + blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
-        const bool f = row_act[i] && cnt[i] == 1 && col_first[sc[i]] == i;
-        fire[i] = f;
-        if (!f) continue;
-        if (__ddiv_rn(rhs[i], sa[i]) < -feas) atomicMin(&ctl->first_bad, i);
-        const int j = sc[i];
-        for (int p = cs[j]; p < cs[j + 1]; ++p) {
-            const int r = ri[p];
-            if (r > i && row_act[r] && cnt[r] >= 2 && fabs(v[p]) > tol) atomicAdd(&hits[r], 1);
-        }
-    }
-}
-
-// the boundary: the first row >= P left with exactly one entry by the
-// tentative singletons below it
-__global__ void kp_boundary(int m, const unsigned char* __restrict__ row_act, const int* __restrict__ cnt,
-                            const int* __restrict__ hits, PsCtl* __restrict__ ctl) {
-    if (ctl->stop) return;
-    const int P = ctl->P;
-    for (int r = P + blockIdx.x * blockDim.x + threadIdx.x; r < m; r += gridDim.x * blockDim.x)
-        if (hits[r] > 0 && row_act[r] && cnt[r] >= 2 && cnt[r] - hits[r] == 1) atomicMin(&ctl->boundary, r);
-}
-
-// flag[i] = singleton committed this round: tentative and below this
-// round's limit L = min(boundary, first negative singleton, m)
-__global__ void kp_fire_flags(int m, const unsigned char* __restrict__ fire, int* __restrict__ flag,
-                              PsCtl* __restrict__ ctl) {
-    const int P = ctl->P;
-    const int L = ctl->stop ? 0 : min(min(ctl->boundary, ctl->first_bad), m);
-    if (blockIdx.x == 0 && threadIdx.x == 0 && !ctl->stop) ctl->L = L;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
-        flag[i] = (i >= P && i < L && fire[i]) ? 1 : 0;
-}
-
-// Commits the singletons below L: records (row singleton, then fixed
-// variable), activity, the fixed value of each column.
-__global__ void kp_commit(int m, const int* __restrict__ scan, const int* __restrict__ sc,
-                          const double* __restrict__ sa, const double* __restrict__ rhs,
-                          const double* __restrict__ obj, unsigned char* __restrict__ row_act,
-                          unsigned char* __restrict__ col_act, int* __restrict__ fix_round, int* __restrict__ fix_row,
-                          double* __restrict__ fix_val, int* __restrict__ fire_col, PsRecords R,
-                          const PsCtl* __restrict__ ctl) {
-    if (ctl->stop) return;
-    const int P = ctl->P, L = ctl->L, round = ctl->round;
-    const long long base = ctl->rec;
-    for (int i = P + blockIdx.x * blockDim.x + threadIdx.x; i < L; i += gridDim.x * blockDim.x) {
-        const int before = i > 0 ? scan[i - 1] : 0;
-        if (scan[i] == before) continue;
-        const int j = sc[i];
-        double fixed = __ddiv_rn(rhs[i], sa[i]);
-        if (fixed < 0.0) fixed = 0.0;
-        const long long t = base + 2LL * before;
-        R.kind[t] = MC_RECORD_ROW_SINGLETON;
-        R.index[t] = i;
-        R.variable[t] = j;
-        R.value[t] = sa[i];
-        R.value2[t] = rhs[i];
-        R.inc_len[t] = 0;
-        R.kind[t + 1] = MC_RECORD_FIXED_VARIABLE;
-        R.index[t + 1] = j;
-        R.variable[t + 1] = -1;
-        R.value[t + 1] = fixed;
-        R.value2[t + 1] = obj[j];
-        row_act[i] = 0;
-        col_act[j] = 0;
-        fix_round[j] = round;
-        fix_row[j] = i;
-        fix_val[j] = fixed;
-        fire_col[before] = j;
-    }
-}
-
-// incident rows of each committed singleton's column (rows active after the
-// commit; 0 past the round's singletons, so that the scan over len is defined)
-__global__ void kp_incident_count(int len, const int* __restrict__ cs, const int* __restrict__ ri, const double* __restrict__ v,
-                                  const unsigned char* __restrict__ row_act, double tol,
-                                  const int* __restrict__ fire_col, const int* __restrict__ fire_scan,
-                                  int* __restrict__ inc_cnt, PsCtl* __restrict__ ctl) {
-    // the round's singletons: the flags below P are 0, so the scan at L-1 counts them
-    const int L = ctl->L;
-    const int nf = (ctl->stop || L <= ctl->P) ? 0 : fire_scan[L - 1];
-    if (blockIdx.x == 0 && threadIdx.x == 0 && !ctl->stop) ctl->nfires = nf;
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < len; q += gridDim.x * blockDim.x) {
-        int c = 0;
-        if (q < nf) {
-            const int j = fire_col[q];
-            for (int p = cs[j]; p < cs[j + 1]; ++p) c += row_act[ri[p]] && fabs(v[p]) > tol;
-        }
-        inc_cnt[q] = c;
-    }
-}
-
-// the incident lists of the round's singletons; marks the rows they touch
-__global__ void kp_incident_fill(const int* __restrict__ cs, const int* __restrict__ ri, const double* __restrict__ v,
-                                 const unsigned char* __restrict__ row_act, double tol,
-                                 const int* __restrict__ fire_col, const int* __restrict__ inc_scan, PsRecords R,
-                                 int* __restrict__ touched, const PsCtl* __restrict__ ctl) {
-    if (ctl->stop) return;
-    const int nf = ctl->nfires, round = ctl->round;
-    const long long base = ctl->rec, ibase = ctl->inc;
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nf; q += gridDim.x * blockDim.x) {
-        const int j = fire_col[q];
-        const long long off = ibase + (q > 0 ? inc_scan[q - 1] : 0);
-        long long w = off;
-        for (int p = cs[j]; p < cs[j + 1]; ++p)
-            if (row_act[ri[p]] && fabs(v[p]) > tol) {
-                R.inc_row[w] = ri[p];
-                R.inc_coef[w] = v[p];
-                touched[ri[p]] = round;
-                ++w;
-            }
-        const long long t = base + 2LL * q + 1;
-        R.inc_off[t] = off;
-        R.inc_len[t] = (int)(w - off);
-    }
-}
-
-// Each row the round's singletons touch applies their fixes in the order of
-// their singleton rows: rhs -= a * fixed (presolve.cpp:155-159), and keeps
-// its count of surviving entries.
-__global__ void kp_substitute(int m, const int* __restrict__ rs, const int* __restrict__ ci,
-                              const double* __restrict__ rv, const int* __restrict__ touched, double tol,
-                              const int* __restrict__ fix_round, const int* __restrict__ fix_row,
-                              const double* __restrict__ fix_val, const unsigned char* __restrict__ col_act,
-                              int* __restrict__ cnt, int* __restrict__ sc, double* __restrict__ sa,
-                              double* __restrict__ rhs, const PsCtl* __restrict__ ctl) {
-    if (ctl->stop || ctl->nfires == 0) return;
-    const int round = ctl->round;
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < m; r += gridDim.x * blockDim.x) {
-        if (touched[r] != round) continue;
-        const int b = rs[r], e = rs[r + 1];
-        int k = 0;
-        for (int p = b; p < e; ++p) k += fix_round[ci[p]] == round && fabs(rv[p]) > tol;
-        if (k == 0) continue;
-        double h = rhs[r];
-        int last = -1;
-        // the row loses k entries; left with one, it records that one
-        const int left = cnt[r] - k;
-        cnt[r] = left;
-        if (left == 1)
-            for (int p = b; p < e; ++p)
-                if (col_act[ci[p]] && fabs(rv[p]) > tol) {
-                    sc[r] = ci[p];
-                    sa[r] = rv[p];
-                }
-        for (int t = 0; t < k; ++t) {  // k fixes, smallest singleton row first
-            int best = kNone;
-            double a = 0.0, f = 0.0;
-            for (int p = b; p < e; ++p) {
-                const int c = ci[p];
-                if (fix_round[c] != round || !(fabs(rv[p]) > tol)) continue;
-                const int fr = fix_row[c];
-                if (fr > last && fr < best) {
-                    best = fr;
-                    a = rv[p];
-                    f = fix_val[c];
+__global__ void __launch_bounds__(kWalkThreads) kp_walk(Walk W) {
+    __shared__ int sh[32];
+    cg::grid_group grid = cg::this_grid();
+    PsCtl* ctl = W.ctl;
+    if (ctl->stop) return;  // set before the launch: the same for every block
+    const int m = W.m, nb = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
+    const int per = (m + nb - 1) / nb;
+    const int lo = min(b * per, m), hi = min(lo + per, m);
+    const double tol = W.tol;
+    for (int it = 0; it <= m; ++it) {
+        const int P = ctl->P, round = ctl->round;
+        const int r0 = max(lo, P);
+        // 1. counts and bids
+        for (int i = r0 + tid; i < hi; i += kWalkThreads) {
+            W.hits[i] = 0;
+            if (it == 0) {
+                int c = 0, j = -1;
+                double a = 0.0;
+                if (W.row_act[i])
+                    for (int p = W.rs[i]; p < W.rs[i + 1]; ++p)
+                        if (W.col_act[W.ci[p]] && fabs(W.rv[p]) > tol) {
+                            ++c;
+                            j = W.ci[p];
+                            a = W.rv[p];
+                        }
+                W.cnt[i] = c;
+                if (c == 1) {
+                    W.sc[i] = j;
+                    W.sa[i] = a;
                 }
             }
-            h = __dsub_rn(h, __dmul_rn(a, f));
-            last = best;
+            if (W.row_act[i] && W.cnt[i] == 1) atomicMin(&W.col_first[W.sc[i]], i);
         }
-        rhs[r] = h;
+        grid.sync();
+        // 2. tentative singletons, hits, first negative value
+        for (int i = r0 + tid; i < hi; i += kWalkThreads) {
+            const bool f = W.row_act[i] && W.cnt[i] == 1 && W.col_first[W.sc[i]] == i;
+            W.fire[i] = f;
+            if (!f) continue;
+            if (__ddiv_rn(W.rhs[i], W.sa[i]) < -W.feas) atomicMin(&ctl->first_bad, i);
+            const int j = W.sc[i];
+            for (int p = W.cs[j]; p < W.cs[j + 1]; ++p) {
+                const int r = W.ri[p];
+                if (r > i && W.row_act[r] && W.cnt[r] >= 2 && fabs(W.v[p]) > tol) atomicAdd(&W.hits[r], 1);
+            }
+        }
+        grid.sync();
+        // 3. boundary; the round's bids are cleared (every bidder had count 1)
+        for (int i = r0 + tid; i < hi; i += kWalkThreads) {
+            if (W.cnt[i] == 1) W.col_first[W.sc[i]] = kNone;
+            const int h = W.hits[i];
+            if (h > 0 && W.row_act[i] && W.cnt[i] >= 2 && W.cnt[i] - h == 1) atomicMin(&ctl->boundary, i);
+        }
+        grid.sync();
+        // 4. the limit; singletons of this block below it
+        const int fb = ctl->first_bad;
+        const int L = min(min(ctl->boundary, fb), m);
+        const long long rec0 = ctl->rec, inc0 = ctl->inc;
+        const int r1 = min(hi, L);
+        int mine = 0, tot = 0;
+        for (int i = r0 + tid; i < r1; i += kWalkThreads) mine += W.fire[i];
+        block_exclusive(mine, sh, &tot);
+        if (tid == 0) W.block_fires[b] = tot;
+        grid.sync();
+        // 5. commit in row order: ranks from the earlier blocks' counts and a block scan
+        int pre = 0, all = 0;
+        for (int q = tid; q < nb; q += kWalkThreads) {
+            const int c = W.block_fires[q];
+            if (q < b) pre += c;
+            all += c;
+        }
+        block_exclusive(pre, sh, &pre);
+        int nf = 0;
+        block_exclusive(all, sh, &nf);
+        const int myfires = W.block_fires[b];
+        int run = 0, my_inc = 0;
+        for (int base = r0; base < r1; base += kWalkThreads) {
+            const int i = base + tid;
+            const int f = (i < r1 && W.fire[i]) ? 1 : 0;
+            int t = 0;
+            const int ex = block_exclusive(f, sh, &t);
+            if (f) {
+                const int q = pre + run + ex;
+                const int j = W.sc[i];
+                double fixed = __ddiv_rn(W.rhs[i], W.sa[i]);
+                if (fixed < 0.0) fixed = 0.0;
+                const long long rt = rec0 + 2LL * q;
+                W.R.kind[rt] = MC_RECORD_ROW_SINGLETON;
+                W.R.index[rt] = i;
+                W.R.variable[rt] = j;
+                W.R.value[rt] = W.sa[i];
+                W.R.value2[rt] = W.rhs[i];
+                W.R.inc_len[rt] = 0;
+                W.R.kind[rt + 1] = MC_RECORD_FIXED_VARIABLE;
+                W.R.index[rt + 1] = j;
+                W.R.variable[rt + 1] = -1;
+                W.R.value[rt + 1] = fixed;
+                W.R.value2[rt + 1] = W.obj[j];
+                W.row_act[i] = 0;
+                W.col_act[j] = 0;
+                W.fix_round[j] = round;
+                W.fix_row[j] = i;
+                W.fix_val[j] = fixed;
+                W.fire_col[q] = j;
+                // the rows this fix reaches: no other singleton of the round
+                // has an entry in column j, so their activity is settled here
+                int c = 0;
+                for (int p = W.cs[j]; p < W.cs[j + 1]; ++p) {
+                    const int r = W.ri[p];
+                    c += r != i && W.row_act[r] && fabs(W.v[p]) > tol;
+                }
+                W.inc_cnt[q] = c;
+                my_inc += c;
+            }
+            run += t;
+        }
+        int inc_tot = 0;
+        block_exclusive(my_inc, sh, &inc_tot);
+        if (tid == 0) W.block_inc[b] = inc_tot;
+        grid.sync();
+        // 6. incident lists (column order), in stack order; touched rows marked
+        int ipre = 0, iall = 0;
+        for (int q = tid; q < nb; q += kWalkThreads) {
+            const int c = W.block_inc[q];
+            if (q < b) ipre += c;
+            iall += c;
+        }
+        block_exclusive(ipre, sh, &ipre);
+        int inc_all = 0;
+        block_exclusive(iall, sh, &inc_all);
+        run = 0;
+        for (int base = 0; base < myfires; base += kWalkThreads) {
+            const int k = base + tid;
+            const int q = pre + k;
+            const int c = k < myfires ? W.inc_cnt[q] : 0;
+            int t = 0;
+            const int ex = block_exclusive(c, sh, &t);
+            if (k < myfires) {
+                const long long off = inc0 + ipre + run + ex;
+                const int j = W.fire_col[q];
+                long long w = off;
+                for (int p = W.cs[j]; p < W.cs[j + 1] && w < off + c; ++p) {
+                    const int r = W.ri[p];
+                    if (W.row_act[r] && fabs(W.v[p]) > tol) {
+                        W.R.inc_row[w] = r;
+                        W.R.inc_coef[w] = W.v[p];
+                        W.touched[r] = round;
+                        ++w;
+                    }
+                }
+                const long long rt = rec0 + 2LL * q + 1;
+                W.R.inc_off[rt] = off;
+                W.R.inc_len[rt] = (int)(w - off);
+            }
+            run += t;
+        }
+        grid.sync();
+        // 7. substitutions in the order of the singleton rows (presolve.cpp:155-159)
+        for (int r = lo + tid; r < hi; r += kWalkThreads) {
+            if (W.touched[r] != round) continue;
+            const int bb = W.rs[r], e = W.rs[r + 1];
+            int k = 0;
+            for (int p = bb; p < e; ++p) k += W.fix_round[W.ci[p]] == round && fabs(W.rv[p]) > tol;
+            if (k == 0) continue;
+            const int left = W.cnt[r] - k;
+            W.cnt[r] = left;
+            if (left == 1)
+                for (int p = bb; p < e; ++p)
+                    if (W.col_act[W.ci[p]] && fabs(W.rv[p]) > tol) {
+                        W.sc[r] = W.ci[p];
+                        W.sa[r] = W.rv[p];
+                    }
+            double h = W.rhs[r];
+            int last = -1;
+            for (int t = 0; t < k; ++t) {  // k fixes, smallest singleton row first
+                int best = kNone;
+                double a = 0.0, f = 0.0;
+                for (int p = bb; p < e; ++p) {
+                    const int c = W.ci[p];
+                    if (W.fix_round[c] != round || !(fabs(W.rv[p]) > tol)) continue;
+                    const int fr = W.fix_row[c];
+                    if (fr > last && fr < best) {
+                        best = fr;
+                        a = W.rv[p];
+                        f = W.fix_val[c];
+                    }
+                }
+                h = __dsub_rn(h, __dmul_rn(a, f));
+                last = best;
+            }
+            W.rhs[r] = h;
+        }
+        if (b == 0 && tid == 0) {  // close the round (the other blocks read no control field until the barrier)
+            ctl->rec = rec0 + 2LL * nf;
+            ctl->inc = inc0 + inc_all;
+            ctl->reductions += nf;
+            ctl->stats[2] += nf;
+            ctl->stats[3] += nf;
+            ctl->round = round + 1;
+            if (fb != kNone && fb == L) {  // presolve.cpp:137-142
+                ctl->stop = 1;
+                ctl->cause = 2;
+                ctl->status = MC_PRESOLVE_INFEASIBLE;
+            } else {
+                ctl->P = L;
+                ctl->boundary = kNone;
+                ctl->first_bad = kNone;
+            }
+        }
+        grid.sync();
+        if (ctl->stop || ctl->P >= m) break;
     }
-}
-
-// resets the column bids of the round (every one-entry row >= P bid)
-__global__ void kp_clear_bids(int m, const int* __restrict__ cnt, const int* __restrict__ sc,
-                              int* __restrict__ col_first, const PsCtl* __restrict__ ctl) {
-    const int P = ctl->P;
-    for (int i = P + blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
-        if (cnt[i] == 1) col_first[sc[i]] = kNone;
-}
-
-__global__ void kp_close_round(int m, const int* __restrict__ inc_scan, PsCtl* __restrict__ ctl) {
-    if (ctl->stop) return;
-    const int nf = ctl->nfires;
-    ctl->inc += nf > 0 ? inc_scan[nf - 1] : 0;
-    ctl->rec += 2LL * nf;
-    ctl->reductions += nf;
-    ctl->stats[2] += nf;
-    ctl->stats[3] += nf;
-    ctl->round += 1;
-    ctl->full = 0;
-    if (ctl->first_bad != kNone && ctl->first_bad == ctl->L) {  // presolve.cpp:137-142
-        ctl->stop = 1;
-        ctl->cause = 2;
-        ctl->status = MC_PRESOLVE_INFEASIBLE;
-        return;
-    }
-    ctl->P = ctl->L;
-    ctl->boundary = kNone;
-    ctl->first_bad = kNone;
 }
 
 __global__ void kp_begin_pass(PsCtl* __restrict__ ctl) {
     ctl->reductions = 0;
-    ctl->full = 1;
     ctl->first_bad = ctl->first_unb = ctl->boundary = kNone;
     ctl->P = 0;
 }
@@ -777,50 +811,18 @@ int presolve_body(Ctx& ctx, const mc_canonical_lp* lp, const mc_presolve_options
     const double tol = o->pivot_tolerance;
     const int gm = blocks_for(ctx, std::max(m, 1), kBlock), gn = blocks_for(ctx, std::max(n, 1), kBlock);
     const PsRecords R = P->R;
-    // One round of the singleton walk (all its sizes are fixed and its scan
-    // position lives on the device), captured once as a graph and replayed.
-    auto enqueue_round = [&]() {
-        kp_single_scan<<<gm, kBlock, 0, s>>>(m, rs, ci, rv, col_act, row_act, tol, cnt, hits, sc, sa, col_first,
-                                             ctl);
-        kp_tentative<<<gm, kBlock, 0, s>>>(m, P->cs, P->ri, P->v, row_act, cnt, hits, sc, sa, col_first, rhs, tol,
-                                           o->feasibility_tolerance, fire, ctl);
-        kp_boundary<<<gm, kBlock, 0, s>>>(m, row_act, cnt, hits, ctl);
-        kp_fire_flags<<<gm, kBlock, 0, s>>>(m, fire, flag, ctl);
-        inclusive_scan(ctx, flag, m, scan_tmp, MC_KERNEL_OTHER);
-        kp_commit<<<gm, kBlock, 0, s>>>(m, flag, sc, sa, rhs, P->obj, row_act, col_act, fix_round, fix_row, fix_val,
-                                        fire_col, R, ctl);
-        kp_incident_count<<<gm, kBlock, 0, s>>>(m, P->cs, P->ri, P->v, row_act, tol, fire_col, flag, inc_cnt,
-                                                ctl);
-        inclusive_scan(ctx, inc_cnt, m, scan_tmp, MC_KERNEL_OTHER);
-        kp_incident_fill<<<gm, kBlock, 0, s>>>(P->cs, P->ri, P->v, row_act, tol, fire_col, inc_cnt, R, touched, ctl);
-        kp_substitute<<<gm, kBlock, 0, s>>>(m, rs, ci, rv, touched, tol, fix_round, fix_row, fix_val, col_act, cnt,
-                                            sc, sa, rhs, ctl);
-        kp_clear_bids<<<gm, kBlock, 0, s>>>(m, cnt, sc, col_first, ctl);
-        kp_close_round<<<1, 1, 0, s>>>(m, inc_cnt, ctl);
-    };
-    cudaGraphExec_t round_graph = nullptr;
-    struct GraphGuard {
-        cudaGraphExec_t* g;
-        ~GraphGuard() {
-            if (*g) cudaGraphExecDestroy(*g);
-        }
-    } graph_guard{&round_graph};
-    auto capture_round = [&]() -> int {
-        CU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        ctx.capturing = true;
-        enqueue_round();
-        ctx.capturing = false;
-        cudaGraph_t g = nullptr;
-        const cudaError_t e = cudaStreamEndCapture(s, &g);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture", __LINE__);
-        const cudaError_t e2 = cudaGraphInstantiate(&round_graph, g, 0);
-        cudaGraphDestroy(g);
-        if (e2 != cudaSuccess) {
-            round_graph = nullptr;
-            return cuda_fail(e2, "cudaGraphInstantiate", __LINE__);
-        }
-        return MC_OK;
-    };
+    // the singleton walk: one cooperative kernel per pass, its grid at most
+    // the co-resident blocks (four per SM at most)
+    int walk_per_sm = 0;
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&walk_per_sm, kp_walk, kWalkThreads, 0));
+    const int walk_blocks = std::max(1, std::min(walk_per_sm, 4)) * ctx.sm_count;
+    int *block_fires = nullptr, *block_inc = nullptr;
+    S.get(&block_fires, (size_t)walk_blocks);
+    S.get(&block_inc, (size_t)walk_blocks);
+    TRY(S.rc);
+    Walk W{m, rs, ci, rv, P->cs, P->ri, P->v, P->obj, row_act, col_act, fire, cnt, hits, sc, col_first, fix_round,
+           fix_row, fire_col, inc_cnt, touched, sa, fix_val, rhs, block_fires, block_inc, tol,
+           o->feasibility_tolerance, R, ctl};
     PsCtl h{};
     long long pass = 0, rounds = 0;
     for (; pass < o->max_passes; ++pass) {
@@ -841,18 +843,18 @@ int presolve_body(Ctx& ctx, const mc_canonical_lp* lp, const mc_presolve_options
             kp_push_cols<<<gn, kBlock, 0, s>>>(n, flag, P->obj, col_act, R, ctl);
             kp_close_step<<<1, 1, 0, s>>>(1, n, flag, ctl);
         }
-        // 3. row singletons (presolve.cpp:119-167), in rounds
-        while (true) {
-            if (m > 0) {
-                if (!round_graph) TRY(capture_round());
-                CU(cudaGraphLaunch(round_graph, s));
-                ++rounds;
-            }
-            CU(cudaMemcpyAsync(&h, ctl, sizeof h, cudaMemcpyDeviceToHost, s));
-            CU(cudaStreamSynchronize(s));
-            TRY(ctx.launch_check("presolve round"));
-            if (m == 0 || h.stop || h.P >= m) break;
+        // 3. row singletons (presolve.cpp:119-167), in rounds on the device
+        if (m > 0) {
+            void* args[] = {&W};
+            ctx.begin_launch(MC_KERNEL_OTHER);
+            CU(cudaLaunchCooperativeKernel((const void*)kp_walk, dim3(walk_blocks), dim3(kWalkThreads), args, 0, s));
+            ctx.end_launch();
         }
+        CU(cudaMemcpyAsync(&h, ctl, sizeof h, cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        TRY(ctx.launch_check("presolve pass"));
+        if (m > 0 && !h.stop && h.P < m) return set_error(MC_ERR_INTERNAL, "presolve: singleton walk did not end");
+        rounds = h.round;
         if (h.stop || h.reductions == 0) break;
     }
     I.empty_rows_removed = h.stats[0];
