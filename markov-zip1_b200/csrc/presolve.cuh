@@ -66,6 +66,8 @@ struct PsCtl {
     int P;          // step 3 scan position
     int round;      // rounds so far (marks the columns fixed in a round)
     int cause;      // what stopped it: 0 empty row, 1 empty column, 2 negative singleton
+    int nhit;       // rows listed in the walk's hit list this round
+    int ntouch;     // rows listed in the walk's touched list this round
     long long rec;   // records on the stack
     long long inc;   // incident entries on the stack
     long long reductions;  // this pass
@@ -186,14 +188,18 @@ __global__ void kp_close_step(int which, int len, const int* __restrict__ scan, 
 // m + 1 rounds; each round commits a singleton or ends the walk).  Phases:
 //   1 counts of the rows >= P (every row in a pass's first round, later the
 //     counts the substitutions keep) and bids of one-entry rows for their
-//     column (atomicMin: the first bidder is the tentative singleton);
-//   2 tentative singletons; hits on the later rows of their columns; the
+//     column (atomicMin: the first bidder is the tentative singleton); each
+//     block lists its bidders in row order;
+//   2 tentative singletons (over the bidder lists); hits on the later rows of
+//     their columns (a row hit for the first time joins the hit list); the
 //     first singleton whose value would be negative;
-//   3 the boundary (first row left with one entry by the hits); bids cleared;
+//   3 the boundary (over the hit list: the first row the hits leave with one
+//     entry); bids cleared;
 //   4 the limit L = min(boundary, first negative, m); singletons per block;
-//   5 commit below L in row order (block prefix + block scan), incident
-//     counts;
-//   6 incident lists in stack order, touched rows marked;
+//     hits cleared;
+//   5 commit below L in row order (block prefix + block scan over the
+//     bidder list), incident counts;
+//   6 incident lists in stack order; touched rows listed;
 //   7 substitutions in the touched rows, counts kept; the round closed.
 struct Walk {
     int m;
@@ -206,6 +212,7 @@ struct Walk {
     int *cnt, *hits, *sc, *col_first, *fix_round, *fix_row, *fire_col, *inc_cnt, *touched;
     double *sa, *fix_val, *rhs;
     int *block_fires, *block_inc;
+    int *bid_list, *hit_list, *touch_list;  // [m] each
     double tol, feas;
     PsRecords R;
     PsCtl* ctl;
@@ -248,65 +255,88 @@ __global__ void __launch_bounds__(kWalkThreads) kp_walk(Walk W) {
     PsCtl* ctl = W.ctl;
     if (ctl->stop) return;  // set before the launch: the same for every block
     const int m = W.m, nb = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
+    const int gtid = b * kWalkThreads + tid, gthreads = nb * kWalkThreads;
     const int per = (m + nb - 1) / nb;
     const int lo = min(b * per, m), hi = min(lo + per, m);
     const double tol = W.tol;
+    int* bids = W.bid_list + lo;  // this block's bidders, ascending (at most hi - lo)
     for (int it = 0; it <= m; ++it) {
         const int P = ctl->P, round = ctl->round;
         const int r0 = max(lo, P);
-        // 1. counts and bids
-        for (int i = r0 + tid; i < hi; i += kWalkThreads) {
-            W.hits[i] = 0;
-            if (it == 0) {
-                int c = 0, j = -1;
-                double a = 0.0;
-                if (W.row_act[i])
-                    for (int p = W.rs[i]; p < W.rs[i + 1]; ++p)
-                        if (W.col_act[W.ci[p]] && fabs(W.rv[p]) > tol) {
-                            ++c;
-                            j = W.ci[p];
-                            a = W.rv[p];
-                        }
-                W.cnt[i] = c;
-                if (c == 1) {
-                    W.sc[i] = j;
-                    W.sa[i] = a;
+        // 1. counts (every row in the pass's first round, later the kept
+        //    counts) and bids; the block's bidders listed in row order
+        int nbid = 0;
+        for (int base = r0; base < hi; base += kWalkThreads) {
+            const int i = base + tid;
+            int f = 0;
+            if (i < hi) {
+                if (it == 0) {
+                    W.hits[i] = 0;
+                    int c = 0, j = -1;
+                    double a = 0.0;
+                    if (W.row_act[i])
+                        for (int p = W.rs[i]; p < W.rs[i + 1]; ++p)
+                            if (W.col_act[W.ci[p]] && fabs(W.rv[p]) > tol) {
+                                ++c;
+                                j = W.ci[p];
+                                a = W.rv[p];
+                            }
+                    W.cnt[i] = c;
+                    if (c == 1) {
+                        W.sc[i] = j;
+                        W.sa[i] = a;
+                    }
                 }
+                f = W.row_act[i] && W.cnt[i] == 1;
             }
-            if (W.row_act[i] && W.cnt[i] == 1) atomicMin(&W.col_first[W.sc[i]], i);
+            int t = 0;
+            const int ex = block_exclusive(f, sh, &t);
+            if (f) {
+                bids[nbid + ex] = i;
+                atomicMin(&W.col_first[W.sc[i]], i);
+            }
+            nbid += t;
         }
         grid.sync();
-        // 2. tentative singletons, hits, first negative value
-        for (int i = r0 + tid; i < hi; i += kWalkThreads) {
-            const bool f = W.row_act[i] && W.cnt[i] == 1 && W.col_first[W.sc[i]] == i;
+        // 2. tentative singletons, hits on the later rows of their columns
+        //    (rows hit for the first time listed), first negative value
+        for (int k = tid; k < nbid; k += kWalkThreads) {
+            const int i = bids[k];
+            const bool f = W.col_first[W.sc[i]] == i;
             W.fire[i] = f;
             if (!f) continue;
             if (__ddiv_rn(W.rhs[i], W.sa[i]) < -W.feas) atomicMin(&ctl->first_bad, i);
             const int j = W.sc[i];
             for (int p = W.cs[j]; p < W.cs[j + 1]; ++p) {
                 const int r = W.ri[p];
-                if (r > i && W.row_act[r] && W.cnt[r] >= 2 && fabs(W.v[p]) > tol) atomicAdd(&W.hits[r], 1);
+                if (r > i && W.row_act[r] && W.cnt[r] >= 2 && fabs(W.v[p]) > tol)
+                    if (atomicAdd(&W.hits[r], 1) == 0) W.hit_list[atomicAdd(&ctl->nhit, 1)] = r;
             }
         }
         grid.sync();
-        // 3. boundary; the round's bids are cleared (every bidder had count 1)
-        for (int i = r0 + tid; i < hi; i += kWalkThreads) {
-            if (W.cnt[i] == 1) W.col_first[W.sc[i]] = kNone;
-            const int h = W.hits[i];
-            if (h > 0 && W.row_act[i] && W.cnt[i] >= 2 && W.cnt[i] - h == 1) atomicMin(&ctl->boundary, i);
+        // 3. boundary (the first row the hits leave with one entry); bids cleared
+        for (int k = tid; k < nbid; k += kWalkThreads) W.col_first[W.sc[bids[k]]] = kNone;
+        const int nhit = ctl->nhit;
+        for (int k = gtid; k < nhit; k += gthreads) {
+            const int r = W.hit_list[k];
+            if (W.cnt[r] - W.hits[r] == 1) atomicMin(&ctl->boundary, r);
         }
         grid.sync();
-        // 4. the limit; singletons of this block below it
+        // 4. the limit; singletons of this block below it; hits cleared
         const int fb = ctl->first_bad;
         const int L = min(min(ctl->boundary, fb), m);
         const long long rec0 = ctl->rec, inc0 = ctl->inc;
-        const int r1 = min(hi, L);
+        for (int k = gtid; k < nhit; k += gthreads) W.hits[W.hit_list[k]] = 0;
         int mine = 0, tot = 0;
-        for (int i = r0 + tid; i < r1; i += kWalkThreads) mine += W.fire[i];
+        for (int k = tid; k < nbid; k += kWalkThreads) {
+            const int i = bids[k];
+            mine += (i < L && W.fire[i]) ? 1 : 0;
+        }
         block_exclusive(mine, sh, &tot);
         if (tid == 0) W.block_fires[b] = tot;
         grid.sync();
-        // 5. commit in row order: ranks from the earlier blocks' counts and a block scan
+        // 5. commit in row order: ranks from the earlier blocks' counts and a
+        //    block scan over the (ascending) bidder list
         int pre = 0, all = 0;
         for (int q = tid; q < nb; q += kWalkThreads) {
             const int c = W.block_fires[q];
@@ -318,9 +348,10 @@ __global__ void __launch_bounds__(kWalkThreads) kp_walk(Walk W) {
         block_exclusive(all, sh, &nf);
         const int myfires = W.block_fires[b];
         int run = 0, my_inc = 0;
-        for (int base = r0; base < r1; base += kWalkThreads) {
-            const int i = base + tid;
-            const int f = (i < r1 && W.fire[i]) ? 1 : 0;
+        for (int base = 0; base < nbid; base += kWalkThreads) {
+            const int k = base + tid;
+            const int i = k < nbid ? bids[k] : 0;
+            const int f = (k < nbid && i < L && W.fire[i]) ? 1 : 0;
             int t = 0;
             const int ex = block_exclusive(f, sh, &t);
             if (f) {
@@ -362,7 +393,7 @@ __global__ void __launch_bounds__(kWalkThreads) kp_walk(Walk W) {
         block_exclusive(my_inc, sh, &inc_tot);
         if (tid == 0) W.block_inc[b] = inc_tot;
         grid.sync();
-        // 6. incident lists (column order), in stack order; touched rows marked
+        // 6. incident lists (column order), in stack order; touched rows listed
         int ipre = 0, iall = 0;
         for (int q = tid; q < nb; q += kWalkThreads) {
             const int c = W.block_inc[q];
@@ -388,7 +419,7 @@ __global__ void __launch_bounds__(kWalkThreads) kp_walk(Walk W) {
                     if (W.row_act[r] && fabs(W.v[p]) > tol) {
                         W.R.inc_row[w] = r;
                         W.R.inc_coef[w] = W.v[p];
-                        W.touched[r] = round;
+                        if (atomicExch(&W.touched[r], round) != round) W.touch_list[atomicAdd(&ctl->ntouch, 1)] = r;
                         ++w;
                     }
                 }
@@ -400,13 +431,14 @@ __global__ void __launch_bounds__(kWalkThreads) kp_walk(Walk W) {
         }
         grid.sync();
         // 7. substitutions in the order of the singleton rows (presolve.cpp:155-159)
-        for (int r = lo + tid; r < hi; r += kWalkThreads) {
-            if (W.touched[r] != round) continue;
+        const int ntouch = ctl->ntouch;
+        for (int k = gtid; k < ntouch; k += gthreads) {
+            const int r = W.touch_list[k];
             const int bb = W.rs[r], e = W.rs[r + 1];
-            int k = 0;
-            for (int p = bb; p < e; ++p) k += W.fix_round[W.ci[p]] == round && fabs(W.rv[p]) > tol;
-            if (k == 0) continue;
-            const int left = W.cnt[r] - k;
+            int kf = 0;
+            for (int p = bb; p < e; ++p) kf += W.fix_round[W.ci[p]] == round && fabs(W.rv[p]) > tol;
+            if (kf == 0) continue;
+            const int left = W.cnt[r] - kf;
             W.cnt[r] = left;
             if (left == 1)
                 for (int p = bb; p < e; ++p)
@@ -416,7 +448,7 @@ __global__ void __launch_bounds__(kWalkThreads) kp_walk(Walk W) {
                     }
             double h = W.rhs[r];
             int last = -1;
-            for (int t = 0; t < k; ++t) {  // k fixes, smallest singleton row first
+            for (int t = 0; t < kf; ++t) {  // kf fixes, smallest singleton row first
                 int best = kNone;
                 double a = 0.0, f = 0.0;
                 for (int p = bb; p < e; ++p) {
@@ -441,6 +473,8 @@ __global__ void __launch_bounds__(kWalkThreads) kp_walk(Walk W) {
             ctl->stats[2] += nf;
             ctl->stats[3] += nf;
             ctl->round = round + 1;
+            ctl->nhit = 0;
+            ctl->ntouch = 0;
             if (fb != kNone && fb == L) {  // presolve.cpp:137-142
                 ctl->stop = 1;
                 ctl->cause = 2;
@@ -816,13 +850,17 @@ int presolve_body(Ctx& ctx, const mc_canonical_lp* lp, const mc_presolve_options
     int walk_per_sm = 0;
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&walk_per_sm, kp_walk, kWalkThreads, 0));
     const int walk_blocks = std::max(1, std::min(walk_per_sm, 4)) * ctx.sm_count;
-    int *block_fires = nullptr, *block_inc = nullptr;
+    int *block_fires = nullptr, *block_inc = nullptr, *bid_list = nullptr, *hit_list = nullptr,
+        *touch_list = nullptr;
     S.get(&block_fires, (size_t)walk_blocks);
     S.get(&block_inc, (size_t)walk_blocks);
+    S.get(&bid_list, mm);
+    S.get(&hit_list, mm);
+    S.get(&touch_list, mm);
     TRY(S.rc);
     Walk W{m, rs, ci, rv, P->cs, P->ri, P->v, P->obj, row_act, col_act, fire, cnt, hits, sc, col_first, fix_round,
-           fix_row, fire_col, inc_cnt, touched, sa, fix_val, rhs, block_fires, block_inc, tol,
-           o->feasibility_tolerance, R, ctl};
+           fix_row, fire_col, inc_cnt, touched, sa, fix_val, rhs, block_fires, block_inc, bid_list, hit_list,
+           touch_list, tol, o->feasibility_tolerance, R, ctl};
     PsCtl h{};
     long long pass = 0, rounds = 0;
     for (; pass < o->max_passes; ++pass) {
