@@ -263,6 +263,13 @@ __global__ void __launch_bounds__(kWalkThreads) kp_walk(Walk W) {
     for (int it = 0; it <= m; ++it) {
         const int P = ctl->P, round = ctl->round;
         const int r0 = max(lo, P);
+        // the lists of the last round are read by every block before the
+        // barrier that ended it, so they restart here (appends come after
+        // the next barrier)
+        if (b == 0 && tid == 0) {
+            ctl->nhit = 0;
+            ctl->ntouch = 0;
+        }
         // 1. counts (every row in the pass's first round, later the kept
         //    counts) and bids; the block's bidders listed in row order
         int nbid = 0;
@@ -466,15 +473,13 @@ __global__ void __launch_bounds__(kWalkThreads) kp_walk(Walk W) {
             }
             W.rhs[r] = h;
         }
-        if (b == 0 && tid == 0) {  // close the round (the other blocks read no control field until the barrier)
+        if (b == 0 && tid == 0) {  // close the round (the other blocks read no control field it writes until the barrier)
             ctl->rec = rec0 + 2LL * nf;
             ctl->inc = inc0 + inc_all;
             ctl->reductions += nf;
             ctl->stats[2] += nf;
             ctl->stats[3] += nf;
             ctl->round = round + 1;
-            ctl->nhit = 0;
-            ctl->ntouch = 0;
             if (fb != kNone && fb == L) {  // presolve.cpp:137-142
                 ctl->stop = 1;
                 ctl->cause = 2;
