@@ -48,6 +48,8 @@
 
 #include <climits>
 #include <cooperative_groups.h>
+#include <map>
+#include <mutex>
 #include <vector>
 
 namespace mc {
@@ -696,35 +698,75 @@ struct mc_presolve {
 
 namespace mc {
 
-inline int ps_alloc(mc_presolve* p, void** ptr, size_t bytes) {
-    if (cudaMalloc(ptr, bytes < 16 ? 16 : bytes) != cudaSuccess) {
+// A stream-ordered memory pool per device for presolve results and scratch.
+// Freed blocks stay reserved (up to 1 GiB) for the next call instead of
+// being unmapped at every synchronisation: repeated presolves then allocate
+// in microseconds.  Pools live until the process exits; where one cannot be
+// made, the device's default pool is used.
+inline cudaMemPool_t ps_pool(int device) {
+    static std::mutex mu;
+    static std::map<int, cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> guard(mu);
+    const auto it = pools.find(device);
+    if (it != pools.end()) return it->second;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+        cudaGetLastError();
+        pool = nullptr;
+    } else {
+        unsigned long long keep = 1ull << 30;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    pools[device] = pool;
+    return pool;
+}
+
+inline cudaError_t ps_malloc(void** ptr, size_t bytes, int device, cudaStream_t s) {
+    const cudaMemPool_t pool = ps_pool(device);
+    return pool ? cudaMallocFromPoolAsync(ptr, bytes, pool, s) : cudaMallocAsync(ptr, bytes, s);
+}
+
+inline int ps_alloc(mc_presolve* p, void** ptr, size_t bytes, cudaStream_t s) {
+    if (ps_malloc(ptr, bytes < 16 ? 16 : bytes, p->device, s) != cudaSuccess) {
         *ptr = nullptr;
+        cudaGetLastError();
         return set_error(MC_ERR_OUT_OF_MEMORY, "presolve buffer (%zu bytes)", bytes);
     }
     p->owned.push_back(*ptr);
     return MC_OK;
 }
 
+// Frees a result: its buffers go back to the pool (ordered on the device's
+// default stream; every call that wrote them has synchronised).
 inline void ps_free(mc_presolve* p) {
     if (!p) return;
     if (p->device >= 0) cudaSetDevice(p->device);
-    for (void* q : p->owned) cudaFree(q);
+    for (void* q : p->owned) cudaFreeAsync(q, 0);
     delete p;
 }
 
+}  // namespace mc
+
+namespace mc {
 
 // Scratch on the context's stream, released when the call ends.
 struct PsScratch {
     cudaStream_t s;
+    int device;
     std::vector<void*> ptrs;
     int rc = MC_OK;
-    explicit PsScratch(cudaStream_t st) : s(st) {}
+    PsScratch(cudaStream_t st, int dev) : s(st), device(dev) {}
     template <class T>
     void get(T** ptr, size_t count) {
         *ptr = nullptr;
         if (rc != MC_OK) return;
-        if (cudaMallocAsync(reinterpret_cast<void**>(ptr), (count < 2 ? 2 : count) * sizeof(T), s) != cudaSuccess) {
+        if (ps_malloc(reinterpret_cast<void**>(ptr), (count < 2 ? 2 : count) * sizeof(T), device, s) != cudaSuccess) {
             *ptr = nullptr;
+            cudaGetLastError();
             rc = set_error(MC_ERR_OUT_OF_MEMORY, "presolve scratch (%zu bytes)", count * sizeof(T));
             return;
         }
@@ -744,7 +786,7 @@ int presolve_body(Ctx& ctx, const mc_canonical_lp* lp, const mc_presolve_options
     {
         int rc = MC_OK;
         auto own = [&](auto** ptr, size_t count) {
-            if (rc == MC_OK) rc = ps_alloc(P, reinterpret_cast<void**>(ptr), count * sizeof(**ptr));
+            if (rc == MC_OK) rc = ps_alloc(P, reinterpret_cast<void**>(ptr), count * sizeof(**ptr), s);
         };
         own(&P->cs, nn);
         own(&P->ri, zz);
@@ -769,7 +811,7 @@ int presolve_body(Ctx& ctx, const mc_canonical_lp* lp, const mc_presolve_options
         own(&P->R.inc_coef, zz);
         TRY(rc);
     }
-    PsScratch S(s);
+    PsScratch S(s, ctx.device);
     const size_t lines = (size_t)std::max(m, n) + 1;
     int *rs, *ci, *cursor, *long_rows, *counters, *scan_tmp, *cnt, *hits, *sc, *col_first, *flag, *fix_round,
         *fix_row, *fire_col, *inc_cnt, *new_row, *cc, *touched;
@@ -1050,7 +1092,7 @@ int presolve_load(Ctx& ctx, const mc_canonical_lp* lp, long long nrec, const int
     const size_t nn = (size_t)n + 1, zz = (size_t)lp->nnz + 1, rr = (size_t)nrec + 1;
     int rc = MC_OK;
     auto own = [&](auto** ptr, size_t count) {
-        if (rc == MC_OK) rc = ps_alloc(P, reinterpret_cast<void**>(ptr), count * sizeof(**ptr));
+        if (rc == MC_OK) rc = ps_alloc(P, reinterpret_cast<void**>(ptr), count * sizeof(**ptr), s);
     };
     own(&P->cs, nn);
     own(&P->ri, zz);
@@ -1100,6 +1142,7 @@ int presolve_load(Ctx& ctx, const mc_canonical_lp* lp, long long nrec, const int
         }();
     }
     if (rc != MC_OK) {
+        cudaStreamSynchronize(s);
         ps_free(P);
         return rc;
     }
@@ -1120,7 +1163,7 @@ int postsolve_body(Ctx& ctx, const mc_presolve* P, const double* rx, long long r
     cudaStream_t s = ctx.stream;
     const int m = P->m, n = P->n;
     const mc_presolve_info& I = P->info;
-    PsScratch S(s);
+    PsScratch S(s, ctx.device);
     double *x, *y, *drx, *dry, *pi_in, *pi_out;
     int *pos, *sing = nullptr, *counters;
     unsigned char *done, *now_done;
