@@ -402,7 +402,9 @@ __global__ void __launch_bounds__(kWalkThreads) kp_walk(Walk W) {
         block_exclusive(my_inc, sh, &inc_tot);
         if (tid == 0) W.block_inc[b] = inc_tot;
         grid.sync();
-        // 6. incident lists (column order), in stack order; touched rows listed
+        // 6. incident lists (column order), in stack order; touched rows listed.
+        //    Offsets per singleton from the block prefix and a block scan, then
+        //    a warp per singleton writes its column's surviving entries.
         int ipre = 0, iall = 0;
         for (int q = tid; q < nb; q += kWalkThreads) {
             const int c = W.block_inc[q];
@@ -415,65 +417,100 @@ __global__ void __launch_bounds__(kWalkThreads) kp_walk(Walk W) {
         run = 0;
         for (int base = 0; base < myfires; base += kWalkThreads) {
             const int k = base + tid;
-            const int q = pre + k;
-            const int c = k < myfires ? W.inc_cnt[q] : 0;
+            const int c = k < myfires ? W.inc_cnt[pre + k] : 0;
             int t = 0;
             const int ex = block_exclusive(c, sh, &t);
             if (k < myfires) {
-                const long long off = inc0 + ipre + run + ex;
-                const int j = W.fire_col[q];
-                long long w = off;
-                for (int p = W.cs[j]; p < W.cs[j + 1] && w < off + c; ++p) {
-                    const int r = W.ri[p];
-                    if (W.row_act[r] && fabs(W.v[p]) > tol) {
-                        W.R.inc_row[w] = r;
-                        W.R.inc_coef[w] = W.v[p];
-                        if (atomicExch(&W.touched[r], round) != round) W.touch_list[atomicAdd(&ctl->ntouch, 1)] = r;
-                        ++w;
-                    }
-                }
-                const long long rt = rec0 + 2LL * q + 1;
-                W.R.inc_off[rt] = off;
-                W.R.inc_len[rt] = (int)(w - off);
+                const long long rt = rec0 + 2LL * (pre + k) + 1;
+                W.R.inc_off[rt] = inc0 + ipre + run + ex;
+                W.R.inc_len[rt] = c;
             }
             run += t;
         }
-        grid.sync();
-        // 7. substitutions in the order of the singleton rows (presolve.cpp:155-159)
-        const int ntouch = ctl->ntouch;
-        for (int k = gtid; k < ntouch; k += gthreads) {
-            const int r = W.touch_list[k];
-            const int bb = W.rs[r], e = W.rs[r + 1];
-            int kf = 0;
-            for (int p = bb; p < e; ++p) kf += W.fix_round[W.ci[p]] == round && fabs(W.rv[p]) > tol;
-            if (kf == 0) continue;
-            const int left = W.cnt[r] - kf;
-            W.cnt[r] = left;
-            if (left == 1)
-                for (int p = bb; p < e; ++p)
-                    if (W.col_act[W.ci[p]] && fabs(W.rv[p]) > tol) {
-                        W.sc[r] = W.ci[p];
-                        W.sa[r] = W.rv[p];
+        __syncthreads();
+        {
+            const int lane = tid & 31;
+            for (int k = tid >> 5; k < myfires; k += kWalkWarps) {
+                const int q = pre + k;
+                const long long rt = rec0 + 2LL * q + 1;
+                long long w = W.R.inc_off[rt];
+                const long long end = w + W.R.inc_len[rt];
+                const int j = W.fire_col[q];
+                for (int p0 = W.cs[j]; p0 < W.cs[j + 1]; p0 += 32) {
+                    const int p = p0 + lane;
+                    bool keep = false;
+                    int r = 0;
+                    if (p < W.cs[j + 1]) {
+                        r = W.ri[p];
+                        keep = W.row_act[r] && fabs(W.v[p]) > tol;
                     }
-            double h = W.rhs[r];
-            int last = -1;
-            for (int t = 0; t < kf; ++t) {  // kf fixes, smallest singleton row first
-                int best = kNone;
-                double a = 0.0, f = 0.0;
-                for (int p = bb; p < e; ++p) {
-                    const int c = W.ci[p];
-                    if (W.fix_round[c] != round || !(fabs(W.rv[p]) > tol)) continue;
-                    const int fr = W.fix_row[c];
-                    if (fr > last && fr < best) {
-                        best = fr;
-                        a = W.rv[p];
-                        f = W.fix_val[c];
+                    const unsigned mask = __ballot_sync(0xffffffffu, keep);
+                    const long long at = w + __popc(mask & ((1u << lane) - 1u));
+                    if (keep && at < end) {
+                        W.R.inc_row[at] = r;
+                        W.R.inc_coef[at] = W.v[p];
+                        if (atomicExch(&W.touched[r], round) != round) W.touch_list[atomicAdd(&ctl->ntouch, 1)] = r;
                     }
+                    w += __popc(mask);
                 }
-                h = __dsub_rn(h, __dmul_rn(a, f));
-                last = best;
             }
-            W.rhs[r] = h;
+        }
+        grid.sync();
+        // 7. substitutions in the order of the singleton rows
+        //    (presolve.cpp:155-159), a warp per touched row: each pass takes
+        //    the round's fix of the smallest singleton row above the last one
+        const int ntouch = ctl->ntouch;
+        {
+            const int lane = tid & 31;
+            for (int k = gtid >> 5; k < ntouch; k += gthreads >> 5) {
+                const int r = W.touch_list[k];
+                const int bb = W.rs[r], e = W.rs[r + 1];
+                int kf = 0;
+                for (int p = bb + lane; p < e; p += 32) kf += W.fix_round[W.ci[p]] == round && fabs(W.rv[p]) > tol;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) kf += __shfl_xor_sync(0xffffffffu, kf, o);
+                if (kf == 0) continue;
+                const int left = W.cnt[r] - kf;
+                if (left == 1)
+                    for (int p = bb + lane; p < e; p += 32)
+                        if (W.col_act[W.ci[p]] && fabs(W.rv[p]) > tol) {
+                            W.sc[r] = W.ci[p];
+                            W.sa[r] = W.rv[p];
+                        }
+                double h = W.rhs[r];
+                int last = -1;
+                for (int t = 0; t < kf; ++t) {
+                    int best = kNone;
+                    double a = 0.0, f = 0.0;
+                    for (int p = bb + lane; p < e; p += 32) {
+                        const int c = W.ci[p];
+                        if (W.fix_round[c] != round || !(fabs(W.rv[p]) > tol)) continue;
+                        const int fr = W.fix_row[c];
+                        if (fr > last && fr < best) {
+                            best = fr;
+                            a = W.rv[p];
+                            f = W.fix_val[c];
+                        }
+                    }
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) {
+                        const int ob = __shfl_xor_sync(0xffffffffu, best, o);
+                        const double oa = __shfl_xor_sync(0xffffffffu, a, o);
+                        const double of = __shfl_xor_sync(0xffffffffu, f, o);
+                        if (ob < best) {
+                            best = ob;
+                            a = oa;
+                            f = of;
+                        }
+                    }
+                    h = __dsub_rn(h, __dmul_rn(a, f));
+                    last = best;
+                }
+                if (lane == 0) {
+                    W.cnt[r] = left;
+                    W.rhs[r] = h;
+                }
+            }
         }
         if (b == 0 && tid == 0) {  // close the round (the other blocks read no control field it writes until the barrier)
             ctl->rec = rec0 + 2LL * nf;
