@@ -402,9 +402,7 @@ __global__ void __launch_bounds__(kWalkThreads) kp_walk(Walk W) {
         block_exclusive(my_inc, sh, &inc_tot);
         if (tid == 0) W.block_inc[b] = inc_tot;
         grid.sync();
-        // 6. incident lists (column order), in stack order; touched rows listed.
-        //    Offsets per singleton from the block prefix and a block scan, then
-        //    a warp per singleton writes its column's surviving entries.
+        // 6. incident lists (column order), in stack order; touched rows listed
         int ipre = 0, iall = 0;
         for (int q = tid; q < nb; q += kWalkThreads) {
             const int c = W.block_inc[q];
@@ -417,43 +415,28 @@ __global__ void __launch_bounds__(kWalkThreads) kp_walk(Walk W) {
         run = 0;
         for (int base = 0; base < myfires; base += kWalkThreads) {
             const int k = base + tid;
-            const int c = k < myfires ? W.inc_cnt[pre + k] : 0;
+            const int q = pre + k;
+            const int c = k < myfires ? W.inc_cnt[q] : 0;
             int t = 0;
             const int ex = block_exclusive(c, sh, &t);
             if (k < myfires) {
-                const long long rt = rec0 + 2LL * (pre + k) + 1;
-                W.R.inc_off[rt] = inc0 + ipre + run + ex;
-                W.R.inc_len[rt] = c;
+                const long long off = inc0 + ipre + run + ex;
+                const int j = W.fire_col[q];
+                long long w = off;
+                for (int p = W.cs[j]; p < W.cs[j + 1] && w < off + c; ++p) {
+                    const int r = W.ri[p];
+                    if (W.row_act[r] && fabs(W.v[p]) > tol) {
+                        W.R.inc_row[w] = r;
+                        W.R.inc_coef[w] = W.v[p];
+                        if (atomicExch(&W.touched[r], round) != round) W.touch_list[atomicAdd(&ctl->ntouch, 1)] = r;
+                        ++w;
+                    }
+                }
+                const long long rt = rec0 + 2LL * q + 1;
+                W.R.inc_off[rt] = off;
+                W.R.inc_len[rt] = (int)(w - off);
             }
             run += t;
-        }
-        __syncthreads();
-        {
-            const int lane = tid & 31;
-            for (int k = tid >> 5; k < myfires; k += kWalkWarps) {
-                const int q = pre + k;
-                const long long rt = rec0 + 2LL * q + 1;
-                long long w = W.R.inc_off[rt];
-                const long long end = w + W.R.inc_len[rt];
-                const int j = W.fire_col[q];
-                for (int p0 = W.cs[j]; p0 < W.cs[j + 1]; p0 += 32) {
-                    const int p = p0 + lane;
-                    bool keep = false;
-                    int r = 0;
-                    if (p < W.cs[j + 1]) {
-                        r = W.ri[p];
-                        keep = W.row_act[r] && fabs(W.v[p]) > tol;
-                    }
-                    const unsigned mask = __ballot_sync(0xffffffffu, keep);
-                    const long long at = w + __popc(mask & ((1u << lane) - 1u));
-                    if (keep && at < end) {
-                        W.R.inc_row[at] = r;
-                        W.R.inc_coef[at] = W.v[p];
-                        if (atomicExch(&W.touched[r], round) != round) W.touch_list[atomicAdd(&ctl->ntouch, 1)] = r;
-                    }
-                    w += __popc(mask);
-                }
-            }
         }
         grid.sync();
         // 7. substitutions in the order of the singleton rows
