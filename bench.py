@@ -435,7 +435,7 @@ def run_presolve_arm(args) -> None:
     import torch
     import mcpdlp
     from mcpdlp import _abi, _lib, _raise, generators
-    from mcpdlp.presolve import CanonicalModel, PresolveOptions, presolve
+    from mcpdlp.presolve import CanonicalModel, PresolveOptions, postsolve, presolve
     world, rank, local = dist_env()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -488,6 +488,14 @@ def run_presolve_arm(args) -> None:
     e2e_s = max_over_ranks(dist, time.perf_counter() - t0, dev)
     red = g.model
     st = g.stack
+    # postsolve of a seeded reduced solution (host arrays in and out)
+    rng = np.random.default_rng(7)
+    sol = type("ReducedSolution", (), {})()
+    sol.primal, sol.dual = rng.uniform(0.0, 2.0, red.num_cols), rng.normal(size=red.num_rows)
+    postsolve(st, sol, c, ctx=ctx)
+    t0 = time.perf_counter()
+    postsolve(st, sol, c, ctx=ctx)
+    post_s = time.perf_counter() - t0
     h2d = c.col_start.nbytes + c.row_index.nbytes + c.value.nbytes + c.rhs.nbytes + c.objective.nbytes
     d2h = sum(a.nbytes for a in (red.col_start, red.row_index, red.value, red.rhs, red.objective, st.kind, st.index,
                                  st.variable, st.value, st.value2, st.incident_start, st.incident_row,
@@ -509,6 +517,7 @@ def run_presolve_arm(args) -> None:
             "presolve": dict(passes_executed=int(info.passes_executed), rounds=int(info.scan_rounds),
                              records=int(info.records), presolved_rows=int(info.presolved_rows),
                              presolved_cols=int(info.presolved_cols), status=int(info.status)),
+            "postsolve_e2e_ms": post_s * 1e3,
             "e2e": {"value": c.nnz / e2e_s, "unit": "nonzeros/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "s_per_step": e2e_s},
             "roofline": {"bound": "hbm", "achieved": algo_bytes / per / 1e9, "peak": hbm, "unit": "GB/s",
