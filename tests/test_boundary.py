@@ -8,6 +8,8 @@ markov-zip1_b200/binding/_build/:
 * pdlp_test -- the reference's tests/pdlp_test.cpp (asserts on).  With
   MARKOV_CERO_PDLP_BACKEND=gpu every solve_pdlp of the process goes to the
   GPU engine; with no visible GPU that must fail loudly (no CPU fallback).
+* ruiz_scaling_test -- the reference's tests/ruiz_scaling_test.cpp with its
+  equilibrate() calls routed to the device (binding/ruiz_gpu.cpp).
 * presolve_test -- the reference's tests/presolve_test.cpp with its
   presolve()/postsolve() calls routed to the device presolve
   (binding/presolve_gpu.cpp); with no visible GPU it must fail loudly.
@@ -38,6 +40,7 @@ BUILD = Path(__file__).resolve().parent.parent / "markov-zip1_b200" / "binding" 
 PDLP_TEST = BUILD / "pdlp_test"
 CLI = BUILD / "markov-cero-solve"
 PRESOLVE_TEST = BUILD / "presolve_test"
+RUIZ_TEST = BUILD / "ruiz_scaling_test"
 
 needs_build = pytest.mark.skipif(not (PDLP_TEST.exists() and CLI.exists()),
                                  reason="integration build absent (needs the reference sources)")
@@ -117,6 +120,13 @@ def test_reference_presolve_test_without_device_fails_loudly():
     assert "no CPU fallback" in (r.stdout + r.stderr)
 
 
+@pytest.mark.skipif(not RUIZ_TEST.exists(), reason="integration build absent (needs the reference sources)")
+def test_reference_ruiz_test_without_device_fails_loudly():
+    r = run([RUIZ_TEST], {"CUDA_VISIBLE_DEVICES": ""})
+    assert r.returncode != 0
+    assert "no CPU fallback" in (r.stdout + r.stderr)
+
+
 @needs_build
 def test_gpu_request_without_device_fails_loudly():
     # a GPU request never falls back to the CPU solver
@@ -170,6 +180,17 @@ def test_reference_presolve_test_on_gpu():
     r = run([PRESOLVE_TEST])
     assert r.returncode == 0, r.stdout + r.stderr
     assert "presolve tests passed" in r.stdout
+
+
+@pytest.mark.skipif(not RUIZ_TEST.exists(), reason="integration build absent (needs the reference sources)")
+@pytest.mark.gpu
+def test_reference_ruiz_test_on_gpu():
+    """tests/ruiz_scaling_test.cpp (asserts on): the equilibrated norms, and
+    the blend model scaled on the device, solved by the reference simplex and
+    unscaled, against the unscaled solve."""
+    r = run([RUIZ_TEST])
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "ruiz scaling tests passed" in r.stdout
 
 
 @needs_build
