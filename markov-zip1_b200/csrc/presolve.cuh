@@ -29,7 +29,8 @@
 //   commits the singletons below B, applies their substitutions, and moves P
 //   to B.  Each round commits at least one singleton or ends the walk, so
 //   rounds <= singletons + 1, and one round suffices when no singleton makes
-//   another.
+//   another.  The rounds of a pass run inside one cooperative kernel
+//   (kp_walk), with grid-wide barriers between their phases.
 // * Substitutions: every row applies the fixes of the round that touch it in
 //   the order of their singleton rows -- the order of the walk -- with the
 //   same operands (rhs -= a * fixed, rounded separately), so the right-hand
