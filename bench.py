@@ -678,10 +678,12 @@ def run_engine_arm(args) -> None:
                                                             / forms["fp32_refine"]["time_to_tol_s"])
 
     # ---- the learned warm start (FP32 + refinement + GNN start, combined): a network
-    # trained on GPU-solved LPs of the same generator at small sizes (m in
-    # [200, 600], n = 3m, 1024 seeds), its dual prediction for this LP fed to
-    # the engine with the guard on (the engine keeps the cold start if the
-    # prediction scores worse); time to 1e-8 includes the prediction
+    # trained on GPU-solved LPs of the same generator at this LP's shape and
+    # small sizes (m in [200, 600], n = 2.5m, 8 per column, 1024 seeds), fed
+    # to the engine as (a) its predicted initial primal weight with the
+    # reference's cold point, and (b) that weight with its predicted dual, the
+    # guard on (the engine keeps the cold point if the prediction scores
+    # worse); time to 1e-8 includes the prediction
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
     hmodel = mcpdlp.Model(m, n, pin(model.col_start), pin(model.row_index), pin(model.value),
                           pin(model.objective), pin(model.var_lower), pin(model.var_upper),
@@ -691,35 +693,39 @@ def run_engine_arm(args) -> None:
         from mcpdlp.learn import WarmStartNet, solve_targets
         t0 = time.perf_counter()
         sizes = [generators.uniform_int(sd, 0, 200, 600) for sd in range(1024)]
-        fam = [generators.random_lp(sd, mm, 3 * mm, 6) for sd, mm in enumerate(sizes)]
+        fam = [generators.random_lp(sd, mm, (5 * mm) // 2, WORKLOAD["k"]) for sd, mm in enumerate(sizes)]
         to = PdlpOptions(device=local, max_iterations=20000)
         to.set_tolerance(1e-8)
         net = WarmStartNet(local, 3, 0)
         net.fit(solve_targets(ctx, fam, to, margin=0.0), epochs=6, lr=2e-3)
         train_s = time.perf_counter() - t0
-        for name, prec in (("fp32_refine_learned_warm", Precision.fp32_refine),):
+        for name, with_dual in (("fp32_refine_learned_weight", False), ("fp32_refine_learned_weight_dual", True)):
             if over_budget():
                 forms[name] = {"skipped": f"wall budget of {args.budget_s:.0f} s reached"}
                 continue
 
-            def warm_solve(prec=prec):
-                # the predicted dual only: on the generator's small LPs the dual half
-                # carries the gain (-6% iterations against -1% for the primal half),
-                # and starts with the predicted primal stalled on this LP
-                _, py, _ = net.predict(hmodel)
-                o = options(prec, warm_start_guard=True)
-                o.initial_dual = py
+            predicted = {}
+
+            def warm_solve(with_dual=with_dual, predicted=predicted):
+                _, py, lw = net.predict(hmodel)
+                o = options(Precision.fp32_refine, warm_start_guard=with_dual)
+                o.initial_primal_weight = predicted["w"] = float(min(max(math.exp(lw), 1e-6), 1e6))
+                if with_dual:
+                    o.initial_dual = py
                 return ctx.solve(hmodel, o)
             r, el, wall = timed_solve(ctx, torch, stream, dist, dev, warm_solve)
             forms[name] = {"time_to_tol_s": wall, "iterations": r.iterations, "status": r.status.name,
                            "objective_rel_err_vs_analytic": abs(r.objective - optimum) / abs(optimum),
                            "warm_start_used": r.extra["warm_start_used"],
-                           "start_score": {"prediction": r.extra["warm_start_score"],
-                                           "cold": r.extra["cold_start_score"]},
-                           "start": "predicted dual, primal from the reference's cold start",
-                           "includes": "prediction (host model), guard, H2D/D2H and the solve",
+                           "initial_primal_weight": predicted.get("w"),
+                           "start": ("predicted dual and primal weight, primal from the reference's cold start"
+                                     if with_dual else "predicted primal weight, the reference's cold point"),
+                           "includes": "prediction (host model), H2D/D2H and the solve",
                            "training_s": train_s, "training": "1024 GPU-solved LPs of the generator at "
-                                                               "m in [200,600], n = 3m, 6 epochs"}
+                                                               "m in [200,600], n = 2.5m, 8 per column, 6 epochs"}
+            if with_dual:
+                forms[name]["start_score"] = {"prediction": r.extra["warm_start_score"],
+                                              "cold": r.extra["cold_start_score"]}
             if "time_to_tol_s" in forms.get("fp64", {}):
                 forms[name]["speedup_time_to_1e-8_vs_fp64"] = forms["fp64"]["time_to_tol_s"] / wall
 

@@ -120,6 +120,20 @@ def test_solve_warm_runs_to_the_same_tolerance(gpu_ctx):
     assert math.isfinite(r.extra["warm_start_score"]) or not r.extra["warm_start_used"]
 
 
+def test_predicted_weight_form_runs_to_the_same_tolerance(gpu_ctx, oracle):
+    """halves="weight": the reference's cold point with the predicted initial
+    primal weight (initial_primal_weight, pdlp.hpp:31) -- same optimum."""
+    net = WarmStartNet(0, 3, 0)
+    m = generators.random_lp(5, 200, 600, 6)
+    o = PdlpOptions(max_iterations=100000)
+    o.set_tolerance(1e-8)
+    r = solve_warm(gpu_ctx, net, m, o, halves="weight")
+    assert r.status == PdlpStatus.optimal
+    assert max(r.primal_infeasibility, r.dual_infeasibility, r.duality_gap) <= 1e-8
+    assert abs(r.objective - m.info["optimum"]) <= 1e-6 * abs(m.info["optimum"])
+    assert not r.extra["warm_start_used"]
+
+
 def test_trained_network_gains_over_untrained_and_cold(gpu_ctx):
     """What training buys, on held-out instances: the trained network's
     prediction starts closer to optimality (the reference's KKT score, as the
