@@ -352,13 +352,25 @@ class Context:
     def solve_device(self, dlp: "DeviceModel", options: Optional[PdlpOptions] = None,
                      primal_out=None, dual_out=None) -> PdlpResult:
         """solve_pdlp on a device-resident model (torch CUDA tensors); the
-        unscaled averages are written to primal_out / dual_out (device)."""
+        unscaled averages are written to primal_out / dual_out (device).
+        options.initial_primal / initial_dual, when given, must be torch CUDA
+        tensors on the model's device (float64, n and m entries)."""
         options = options or PdlpOptions()
         o = options.to_struct()
         lp = dlp.to_struct()
         res = _abi.McPdlpResult()
+        starts = []
+        for v, size in ((options.initial_primal, dlp.num_cols), (options.initial_dual, dlp.num_rows)):
+            if v is None:
+                starts.append(None)
+                continue
+            if not hasattr(v, "data_ptr") or not getattr(v, "is_cuda", False):
+                raise ValueError("a device model takes device (torch CUDA) starting points")
+            if tuple(v.shape) != (size,) or str(v.dtype) != "torch.float64" or not v.is_contiguous():
+                raise ValueError("starting point must be a contiguous float64 tensor of the model's size")
+            starts.append(v.data_ptr())
         rc = self._lib.mc_pdlp_ctx_solve(
-            self._h, C.addressof(lp), C.addressof(o), None, None,
+            self._h, C.addressof(lp), C.addressof(o), starts[0], starts[1],
             None if primal_out is None else primal_out.data_ptr(),
             None if dual_out is None else dual_out.data_ptr(), C.addressof(res), None)
         _raise(rc)

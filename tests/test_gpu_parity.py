@@ -190,6 +190,28 @@ def test_device_resident_input_matches_host(gpu_ctx):
     assert np.array_equal(y.cpu().numpy(), host.dual)
 
 
+def test_device_resident_warm_start_matches_host(gpu_ctx):
+    """A device model takes device starting points; the result equals the
+    host solve from the same points (and host arrays are refused)."""
+    import dataclasses
+    import torch
+    m = synthetic("config0_s3")
+    cold = gpu_ctx.solve(m, gpu_opts(1e-8))
+    x0, y0 = 0.9 * cold.primal, 0.9 * cold.dual
+    ho = gpu_opts(1e-8)
+    ho.initial_primal, ho.initial_dual = x0, y0
+    host = gpu_ctx.solve(m, ho)
+    dm = mcpdlp.DeviceModel(m)
+    do = dataclasses.replace(ho, initial_primal=torch.from_numpy(x0).cuda(), initial_dual=torch.from_numpy(y0).cuda())
+    x = torch.zeros(m.num_cols, dtype=torch.float64, device="cuda")
+    y = torch.zeros(m.num_rows, dtype=torch.float64, device="cuda")
+    dev = gpu_ctx.solve_device(dm, do, x, y)
+    assert dev.iterations == host.iterations and dev.objective == host.objective
+    assert np.array_equal(y.cpu().numpy(), host.dual)
+    with pytest.raises(ValueError):
+        gpu_ctx.solve_device(dm, ho)
+
+
 def test_nonfinite_objective_is_numerical_failure(gpu_ctx):
     """NaN data ends as numerical_failure (the reference would run on to its
     iteration limit on NaNs; the engine stops at the next check)."""
