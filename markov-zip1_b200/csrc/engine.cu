@@ -189,6 +189,43 @@ int pick_lanes(double mean_len) {
 #include "verify.cuh"
 #include "presolve.cuh"
 
+namespace mc {
+// The learned warm start's large instances use the engine's device transpose
+// (rows in ascending column order): an auxiliary context and the CSR of a
+// device CSC.  Declared in gnn.cu.
+Ctx* aux_ctx_create(int device) {
+    Ctx* c = new Ctx();
+    if (c->init(device) != MC_OK) {
+        delete c;
+        return nullptr;
+    }
+    return c;
+}
+
+void aux_ctx_destroy(Ctx* c) { delete c; }
+
+int aux_csr(Ctx* c, int m, int n, long long nnz, const int* cs, const int* ri, const double* v, int* rs, int* ci,
+            double* rv) {
+    cudaStream_t s = c->stream;
+    int *cursor = nullptr, *long_rows = nullptr, *counters = nullptr, *scan = nullptr;
+    const size_t scan_ints = (size_t)(m + 1) / kScanTile + 4096;
+    int rc = MC_OK;
+    auto get = [&](int** p, size_t count) {
+        if (rc == MC_OK && cudaMallocAsync(reinterpret_cast<void**>(p), sizeof(int) * count, s) != cudaSuccess)
+            rc = set_error(MC_ERR_OUT_OF_MEMORY, "transpose scratch");
+    };
+    get(&cursor, (size_t)m + 1);
+    get(&long_rows, (size_t)m + 1);
+    get(&counters, 4);
+    get(&scan, scan_ints);
+    if (rc == MC_OK) rc = build_csr(*c, m, n, nnz, cs, ri, v, rs, ci, rv, cursor, long_rows, counters, scan);
+    for (int* p : {cursor, long_rows, counters, scan})
+        if (p) cudaFreeAsync(p, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess && rc == MC_OK) rc = set_error(MC_ERR_CUDA, "transpose");
+    return rc;
+}
+}  // namespace mc
+
 using namespace mc;
 
 // =================================================================== C ABI

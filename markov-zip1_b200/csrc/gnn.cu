@@ -27,11 +27,19 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <vector>
 
 namespace mc {
 int set_error(int code, const char* fmt, ...);
+struct Ctx;
+Ctx* aux_ctx_create(int device);
+void aux_ctx_destroy(Ctx* c);
+int aux_csr(Ctx* c, int m, int n, long long nnz, const int* cs, const int* ri, const double* v, int* rs, int* ci,
+            double* rv);
 }
 
 namespace {
@@ -349,6 +357,34 @@ int tile_grid(long long rows) {
 }
 
 // One instance on the device: graph, features, activations, gradients.
+// A stream-ordered memory pool per device for instance buffers: freed blocks
+// stay reserved (up to 2 GiB) for the next instance, so that a call on a large
+// LP does not map and unmap its buffers every time.  Lives until exit; where
+// one cannot be made, the device's default pool is used.
+cudaMemPool_t instance_pool(int device) {
+    static std::mutex mu;
+    static std::map<int, cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> guard(mu);
+    const auto it = pools.find(device);
+    if (it != pools.end()) return it->second;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+        cudaGetLastError();
+        pool = nullptr;
+    } else {
+        unsigned long long keep = 2ull << 30;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    pools[device] = pool;
+    return pool;
+}
+
+// Buffers of one instance, on the network's stream; freed (stream-ordered)
+// when the instance goes away.
 struct Instance {
     int m = 0, n = 0;
     long long nnz = 0;
@@ -356,14 +392,19 @@ struct Instance {
     float *cv = nullptr, *rv = nullptr, *rinv = nullptr, *cinv = nullptr;
     float *Fv = nullptr, *Fc = nullptr;
     double bscale = 1.0, cscale = 1.0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
     std::vector<void*> owned;
+    Instance(int dev, cudaStream_t s) : device(dev), stream(s) {}
     ~Instance() {
-        for (void* p : owned) cudaFree(p);
+        for (void* p : owned) cudaFreeAsync(p, stream);
     }
     template <class T>
     int alloc(T** p, long long count) {
         void* q = nullptr;
-        GCU(cudaMalloc(&q, sizeof(T) * (size_t)std::max<long long>(count, 1)));
+        const size_t bytes = sizeof(T) * (size_t)std::max<long long>(count, 1);
+        const cudaMemPool_t pool = instance_pool(device);
+        GCU(pool ? cudaMallocFromPoolAsync(&q, bytes, pool, stream) : cudaMallocAsync(&q, bytes, stream));
         owned.push_back(q);
         *p = static_cast<T*>(q);
         return MC_OK;
@@ -391,8 +432,10 @@ struct mc_gnn {
     double* dpart = nullptr;
     long long cap_n = -1, cap_m = -1;
     std::vector<void*> ws;
+    mc::Ctx* aux = nullptr;  // the engine's transpose, for large instances
     ~mc_gnn() {
         if (device >= 0) cudaSetDevice(device);
+        if (aux) mc::aux_ctx_destroy(aux);
         for (void* p : ws) cudaFree(p);
         cudaFree(params);
         cudaFree(grads);
@@ -451,8 +494,172 @@ int reserve_ws(mc_gnn* g, int n, int m) {
     return MC_OK;
 }
 
+
+// ------------------------------------------------- instance on the device
+// The same graph and features as the host build (bit for bit: the same
+// float sums in the same order -- a column over its entries, a row over its
+// columns in ascending order -- and the same double/float conversions).
+__global__ void g_col_norms(int n, const int* __restrict__ cs, const double* __restrict__ v, float* __restrict__ cv,
+                            float* __restrict__ cnorm) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        float acc = 0.f;
+        for (int p = cs[j]; p < cs[j + 1]; ++p) {
+            cv[p] = (float)v[p];
+            acc += (float)fabs(v[p]);
+        }
+        cnorm[j] = acc;
+    }
+}
+
+__global__ void g_row_norms(int m, const int* __restrict__ rs, const double* __restrict__ rvd, float* __restrict__ rv,
+                            float* __restrict__ rnorm) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        float acc = 0.f;
+        for (int p = rs[i]; p < rs[i + 1]; ++p) {
+            rv[p] = (float)rvd[p];
+            acc += (float)fabs(rvd[p]);
+        }
+        rnorm[i] = acc;
+    }
+}
+
+// max of non-negative floats (their bit patterns order like the values)
+__global__ void g_max_nonneg(long long len, const float* __restrict__ a, unsigned* __restrict__ out) {
+    unsigned best = 0u;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len; i += (long long)gridDim.x * blockDim.x)
+        best = max(best, __float_as_uint(a[i]));
+    for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, best);
+}
+
+__global__ void g_var_features(int n, const double* __restrict__ obj, const double* __restrict__ lo,
+                               const double* __restrict__ hi, const float* __restrict__ cnorm,
+                               const unsigned* __restrict__ cmax_bits, double bs, double cs, float* __restrict__ Fv,
+                               float* __restrict__ cinv) {
+    const float cmax = fmaxf(1e-30f, __uint_as_float(*cmax_bits));
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const double l = lo[j], h = hi[j];
+        float* f = Fv + (size_t)j * FV;
+        f[0] = (float)(obj[j] / cs);
+        f[1] = isfinite(l) ? 1.f : 0.f;
+        f[2] = isfinite(h) ? 1.f : 0.f;
+        f[3] = isfinite(l) ? (float)fmax(-10.0, fmin(10.0, l / bs)) : 0.f;
+        f[4] = isfinite(h) ? (float)fmax(-10.0, fmin(10.0, h / bs)) : 0.f;
+        f[5] = cnorm[j] / cmax;
+        cinv[j] = cnorm[j] > 0.f ? 1.f / cnorm[j] : 0.f;
+    }
+}
+
+__global__ void g_row_features(int m, const double* __restrict__ lo, const double* __restrict__ hi,
+                               const float* __restrict__ rnorm, const unsigned* __restrict__ rmax_bits, double bs,
+                               float* __restrict__ Fc, float* __restrict__ rinv) {
+    const float rmax = fmaxf(1e-30f, __uint_as_float(*rmax_bits));
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        const double l = lo[i], h = hi[i];
+        float* f = Fc + (size_t)i * FC;
+        f[0] = isfinite(l) ? (float)(l / bs) : 0.f;
+        f[1] = isfinite(h) ? (float)(h / bs) : 0.f;
+        f[2] = isfinite(l) ? 1.f : 0.f;
+        f[3] = isfinite(h) ? 1.f : 0.f;
+        f[4] = rnorm[i] / rmax;
+        rinv[i] = rnorm[i] > 0.f ? 1.f / rnorm[i] : 0.f;
+    }
+}
+
+__global__ void g_check_csc(int m, int n, long long nnz, const int* __restrict__ cs, const int* __restrict__ ri,
+                            int* __restrict__ bad) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const int b = cs[j], e = cs[j + 1];
+        if ((j == 0 && b != 0) || (j == n - 1 && (long long)e != nnz) || b < 0 || b > e || (long long)e > nnz) {
+            atomicOr(bad, 1);
+            continue;
+        }
+        for (int p = b; p < e; ++p)
+            if (ri[p] < 0 || ri[p] >= m) atomicOr(bad, 2);
+    }
+}
+
+// Large instances (at least 2^20 nonzeros; the environment variable
+// MC_GNN_DEVICE_BUILD_MIN_NNZ moves the threshold) are built on the device:
+// the engine's transpose for the CSR, then norms and features in kernels.
+long long device_build_min_nnz() {
+    const char* e = std::getenv("MC_GNN_DEVICE_BUILD_MIN_NNZ");
+    return e ? std::atoll(e) : (1LL << 20);
+}
+
+int load_instance_device(mc_gnn* g, const mc_lp* lp, Instance& I) {
+    cudaStream_t s = g->stream;
+    const int m = I.m, n = I.n;
+    const long long nnz = I.nnz;
+    if (!g->aux) {
+        g->aux = mc::aux_ctx_create(g->device);
+        if (!g->aux) return mc::set_error(MC_ERR_CUDA, "auxiliary context for the network's transpose");
+    }
+    double bs = 1.0, cs = 1.0;  // |b|_inf and |c|_inf, as the host build takes them
+    for (int i = 0; i < m; ++i) {
+        if (std::isfinite(lp->row_lower[i])) bs = std::max(bs, std::fabs(lp->row_lower[i]));
+        if (std::isfinite(lp->row_upper[i])) bs = std::max(bs, std::fabs(lp->row_upper[i]));
+    }
+    for (int j = 0; j < n; ++j) cs = std::max(cs, std::fabs(lp->objective[j]));
+    I.bscale = bs;
+    I.cscale = cs;
+    Instance T(g->device, s);  // staging, freed on return
+    double *v = nullptr, *rvd = nullptr, *obj = nullptr, *vlo = nullptr, *vhi = nullptr, *rlo = nullptr,
+           *rhi = nullptr;
+    float *cnorm = nullptr, *rnorm = nullptr;
+    unsigned* maxes = nullptr;
+    int* bad = nullptr;
+    GTRY(T.alloc(&v, nnz));
+    GTRY(T.alloc(&rvd, nnz));
+    GTRY(T.alloc(&obj, n));
+    GTRY(T.alloc(&vlo, n));
+    GTRY(T.alloc(&vhi, n));
+    GTRY(T.alloc(&rlo, m));
+    GTRY(T.alloc(&rhi, m));
+    GTRY(T.alloc(&cnorm, n));
+    GTRY(T.alloc(&rnorm, m));
+    GTRY(T.alloc(&maxes, 2));
+    GTRY(T.alloc(&bad, 1));
+    GTRY(I.alloc(&I.cs, n + 1));
+    GTRY(I.alloc(&I.ri, nnz));
+    GTRY(I.alloc(&I.cv, nnz));
+    GTRY(I.alloc(&I.rs, m + 1));
+    GTRY(I.alloc(&I.ci, nnz));
+    GTRY(I.alloc(&I.rv, nnz));
+    GTRY(I.alloc(&I.rinv, m));
+    GTRY(I.alloc(&I.cinv, n));
+    GTRY(I.alloc(&I.Fv, (long long)n * FV));
+    GTRY(I.alloc(&I.Fc, (long long)m * FC));
+    GCU(cudaMemcpyAsync(I.cs, lp->col_start, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s));
+    GCU(cudaMemcpyAsync(I.ri, lp->row_index, sizeof(int) * nnz, cudaMemcpyHostToDevice, s));
+    GCU(cudaMemcpyAsync(v, lp->value, sizeof(double) * nnz, cudaMemcpyHostToDevice, s));
+    GCU(cudaMemcpyAsync(obj, lp->objective, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    GCU(cudaMemcpyAsync(vlo, lp->var_lower, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    GCU(cudaMemcpyAsync(vhi, lp->var_upper, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    GCU(cudaMemcpyAsync(rlo, lp->row_lower, sizeof(double) * m, cudaMemcpyHostToDevice, s));
+    GCU(cudaMemcpyAsync(rhi, lp->row_upper, sizeof(double) * m, cudaMemcpyHostToDevice, s));
+    GCU(cudaMemsetAsync(bad, 0, sizeof(int), s));
+    GCU(cudaMemsetAsync(maxes, 0, sizeof(unsigned) * 2, s));
+    g_check_csc<<<grid_of(n), kThreads, 0, s>>>(m, n, nnz, I.cs, I.ri, bad);
+    int hb = 0;
+    GCU(cudaMemcpyAsync(&hb, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+    GCU(cudaStreamSynchronize(s));
+    if (hb) return mc::set_error(MC_ERR_INVALID_ARGUMENT, hb & 2 ? "row index out of range" : "invalid CSC offsets");
+    GTRY(mc::aux_csr(g->aux, m, n, nnz, I.cs, I.ri, v, I.rs, I.ci, rvd));
+    g_col_norms<<<grid_of(n), kThreads, 0, s>>>(n, I.cs, v, I.cv, cnorm);
+    g_row_norms<<<grid_of(m), kThreads, 0, s>>>(m, I.rs, rvd, I.rv, rnorm);
+    g_max_nonneg<<<grid_of(n), kThreads, 0, s>>>(n, cnorm, maxes);
+    g_max_nonneg<<<grid_of(m), kThreads, 0, s>>>(m, rnorm, maxes + 1);
+    g_var_features<<<grid_of(n), kThreads, 0, s>>>(n, obj, vlo, vhi, cnorm, maxes, bs, cs, I.Fv, I.cinv);
+    g_row_features<<<grid_of(m), kThreads, 0, s>>>(m, rlo, rhi, rnorm, maxes + 1, bs, I.Fc, I.rinv);
+    GCU(cudaGetLastError());
+    GCU(cudaStreamSynchronize(s));  // the staging buffers are freed on return
+    return MC_OK;
+}
+
 // Graph and features of an LP given in host memory.
-int load_instance(const mc_lp* lp, Instance& I, cudaStream_t s) {
+int load_instance(mc_gnn* g, const mc_lp* lp, Instance& I) {
+    cudaStream_t s = g->stream;
     if (!lp || lp->memory != MC_MEMORY_HOST)
         return mc::set_error(MC_ERR_INVALID_ARGUMENT, "the network reads LPs from host memory");
     const int m = lp->num_rows, n = lp->num_cols;
@@ -461,6 +668,7 @@ int load_instance(const mc_lp* lp, Instance& I, cudaStream_t s) {
     I.m = m;
     I.n = n;
     I.nnz = nnz;
+    if (nnz >= device_build_min_nnz()) return load_instance_device(g, lp, I);
     // host: CSR (stable counting sort keeps columns ascending), norms, features
     std::vector<int> rs(m + 1, 0), ci(nnz);
     std::vector<float> rv(nnz), cv(nnz), rnorm(m, 0.f), cnorm(n, 0.f);
@@ -804,8 +1012,8 @@ int mc_gnn_set_params(mc_gnn* g, const float* host_in) {
 int mc_gnn_predict(mc_gnn* g, const mc_lp* lp, double* x_out, double* y_out, double* log_omega_out) {
     if (!g) return mc::set_error(MC_ERR_INVALID_ARGUMENT, "network is NULL");
     Guard guard(g->device);
-    Instance I;
-    GTRY(load_instance(lp, I, g->stream));
+    Instance I(g->device, g->stream);
+    GTRY(load_instance(g, lp, I));
     GTRY(reserve_ws(g, I.n, I.m));
     GTRY(forward(g, I));
     std::vector<float> px(I.n), py(I.m);
@@ -825,8 +1033,8 @@ int mc_gnn_loss_and_grad(mc_gnn* g, const mc_lp* lp, const double* x_target, con
                          double log_omega_target, double* loss, float* grad_out) {
     if (!g || !x_target || !y_target || !loss) return mc::set_error(MC_ERR_INVALID_ARGUMENT, "bad arguments");
     Guard guard(g->device);
-    Instance I;
-    GTRY(load_instance(lp, I, g->stream));
+    Instance I(g->device, g->stream);
+    GTRY(load_instance(g, lp, I));
     GTRY(reserve_ws(g, I.n, I.m));
     GTRY(set_targets(g, I, x_target, y_target));
     GTRY(loss_and_grad(g, I, log_omega_target, loss));

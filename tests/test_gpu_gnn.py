@@ -120,6 +120,24 @@ def test_solve_warm_runs_to_the_same_tolerance(gpu_ctx):
     assert math.isfinite(r.extra["warm_start_score"]) or not r.extra["warm_start_used"]
 
 
+def test_device_built_instance_matches_host_build(gpu_ctx, monkeypatch):
+    """Large LPs are built on the device (the engine's transpose, norms and
+    features in kernels); the result must be the host build's, bit for bit."""
+    m = generators.random_lp(8, 3000, 9000, 6)
+    net = WarmStartNet(0, 3, 0)
+    monkeypatch.setenv("MC_GNN_DEVICE_BUILD_MIN_NNZ", str(1 << 40))
+    xh, yh, wh = net.predict(m)
+    monkeypatch.setenv("MC_GNN_DEVICE_BUILD_MIN_NNZ", "0")
+    xd, yd, wd = net.predict(m)
+    assert np.array_equal(xh, xd) and np.array_equal(yh, yd) and wh == wd
+    t = solve_targets(gpu_ctx, [m], PdlpOptions(max_iterations=2000), margin=0.0)[0]
+    monkeypatch.setenv("MC_GNN_DEVICE_BUILD_MIN_NNZ", str(1 << 40))
+    lh, gh = net.loss_and_grad(t)
+    monkeypatch.setenv("MC_GNN_DEVICE_BUILD_MIN_NNZ", "0")
+    ld, gd = net.loss_and_grad(t)
+    assert lh == ld and np.array_equal(gh, gd)
+
+
 def test_predicted_weight_form_runs_to_the_same_tolerance(gpu_ctx, oracle):
     """halves="weight": the reference's cold point with the predicted initial
     primal weight (initial_primal_weight, pdlp.hpp:31) -- same optimum."""
