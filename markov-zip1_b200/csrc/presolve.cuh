@@ -914,10 +914,11 @@ int presolve_body(Ctx& ctx, const mc_canonical_lp* lp, const mc_presolve_options
     const int gm = blocks_for(ctx, std::max(m, 1), kBlock), gn = blocks_for(ctx, std::max(n, 1), kBlock);
     const PsRecords R = P->R;
     // the singleton walk: one cooperative kernel per pass, its grid at most
-    // the co-resident blocks (four per SM at most)
+    // the co-resident blocks (four per SM at most), and no more than one per
+    // 512 rows: a small model's barriers then span few blocks
     int walk_per_sm = 0;
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&walk_per_sm, kp_walk, kWalkThreads, 0));
-    const int walk_blocks = std::max(1, std::min(walk_per_sm, 4)) * ctx.sm_count;
+    const int walk_blocks = std::max(1, std::min(std::max(1, std::min(walk_per_sm, 4)) * ctx.sm_count, (m + 511) / 512));
     int *block_fires = nullptr, *block_inc = nullptr, *bid_list = nullptr, *hit_list = nullptr,
         *touch_list = nullptr;
     S.get(&block_fires, (size_t)walk_blocks);
