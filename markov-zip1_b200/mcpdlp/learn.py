@@ -175,9 +175,10 @@ def solve_warm(ctx: Context, net: WarmStartNet, model: Model, options: PdlpOptio
     the predicted weight too.  halves: "both", "dual" (the predicted dual with
     the cold primal start), "primal", or "weight" (the reference's cold point
     with the predicted weight; nothing to guard).  On the 40M-nonzero LP of
-    the same generator the predicted weight is the half that pays: from the
-    cold point it reached 1e-8 in 26,560-37,200 iterations against 60,480
-    with the derived weight."""
+    the generator's seed 1 the predicted weight is the half that pays: from
+    the cold point it reached 1e-8 in 26,560-37,200 iterations against 60,480
+    with the derived weight; on seeds 2 and 3 at the same size it changed the
+    count by +1% and -5%."""
     if halves not in ("both", "dual", "primal", "weight"):
         raise ValueError("halves must be 'both', 'dual', 'primal' or 'weight'")
     x, y, lw = net.predict(model)
