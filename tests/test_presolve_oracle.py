@@ -159,3 +159,17 @@ def test_empty_models(oracle, reference):
               CanonicalModel(3, 0, [0], [], [], [0.0, 0.0, 0.0], []),
               CanonicalModel(0, 2, [0, 0, 0], [], [], [], [1.0, 2.0])):
         same(oracle.presolve(c), reference.presolve(c))
+
+
+def test_presolve_workload_is_seeded_and_valid(oracle):
+    """The timing workload's generator (bench.py --workload presolve, at a
+    small size): the same arrays for the same seed, a model the reference's
+    validate() accepts, and every reduction kind present."""
+    a = generators.presolve_workload(3, 20000, 30000, k=3, chains=8, chain_len=10)
+    b = generators.presolve_workload(3, 20000, 30000, k=3, chains=8, chain_len=10)
+    assert canonical_digest(a) == canonical_digest(b)
+    res = oracle.presolve(a)
+    assert res.status == SolveStatus.optimal
+    st = res.statistics
+    assert st.empty_rows_removed > 0 and st.empty_cols_removed > 0 and st.row_singletons_removed > 0
+    assert st.passes_executed >= 2
