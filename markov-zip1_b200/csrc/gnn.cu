@@ -270,11 +270,30 @@ __global__ void g_readout(int N, const float* __restrict__ X, const float* __res
     }
 }
 
-// column means of X [N x H] -> out[H] (one block)
-__global__ void g_col_mean(int N, const float* __restrict__ X, float* __restrict__ out) {
+// column means of X [N x H] -> out[H], in two fixed-order stages: each
+// block sums a contiguous row range (4 row groups of H columns, combined in
+// order), then one block adds the block sums in block order
+constexpr int kMeanBlocks = 512;
+__global__ void g_col_sum_parts(int N, const float* __restrict__ X, double* __restrict__ parts) {
+    __shared__ double sh[kThreads];
+    const int c = threadIdx.x % H, grp = threadIdx.x / H, ngrp = kThreads / H;
+    const long long per = ((long long)N + gridDim.x - 1) / gridDim.x;
+    const long long r0 = blockIdx.x * per, r1 = min((long long)N, r0 + per);
+    double acc = 0.0;
+    for (long long r = r0 + grp; r < r1; r += ngrp) acc += X[r * H + c];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    if (grp == 0) {
+        double t = sh[c];
+        for (int q = 1; q < ngrp; ++q) t += sh[q * H + c];
+        parts[(long long)blockIdx.x * H + c] = t;
+    }
+}
+
+__global__ void g_col_mean(int N, int nparts, const double* __restrict__ parts, float* __restrict__ out) {
     for (int c = threadIdx.x; c < H; c += blockDim.x) {
         double acc = 0.0;
-        for (int r = 0; r < N; ++r) acc += X[(long long)r * H + c];
+        for (int b = 0; b < nparts; ++b) acc += parts[(long long)b * H + c];
         out[c] = (float)(acc / (N > 0 ? N : 1));
     }
 }
@@ -430,6 +449,7 @@ struct mc_gnn {
     float *dhv = nullptr, *dhc = nullptr, *dhv2 = nullptr, *dhc2 = nullptr, *dag = nullptr;
     float *part = nullptr;
     double* dpart = nullptr;
+    double* mpart = nullptr;  // block sums of the readout's column means
     long long cap_n = -1, cap_m = -1;
     std::vector<void*> ws;
     mc::Ctx* aux = nullptr;  // the engine's transpose, for large instances
@@ -489,6 +509,10 @@ int reserve_ws(mc_gnn* g, int n, int m) {
     GCU(cudaMalloc(&q, sizeof(double) * 4096));
     g->ws.push_back(q);
     g->dpart = static_cast<double*>(q);
+    q = nullptr;
+    GCU(cudaMalloc(&q, sizeof(double) * kMeanBlocks * H));
+    g->ws.push_back(q);
+    g->mpart = static_cast<double*>(q);
     g->cap_n = n;
     g->cap_m = m;
     return MC_OK;
@@ -770,8 +794,10 @@ int forward(mc_gnn* g, const Instance& I) {
     const int R = g->rounds;
     g_readout<<<grid_of(n), kThreads, 0, s>>>(n, g->hv[R], P + L.wx, P + L.bx, g->px);
     g_readout<<<grid_of(m), kThreads, 0, s>>>(m, g->hc[R], P + L.wy, P + L.by, g->py);
-    g_col_mean<<<1, H, 0, s>>>(n, g->hv[R], g->mv);
-    g_col_mean<<<1, H, 0, s>>>(m, g->hc[R], g->mcm);
+    g_col_sum_parts<<<kMeanBlocks, kThreads, 0, s>>>(n, g->hv[R], g->mpart);
+    g_col_mean<<<1, H, 0, s>>>(n, kMeanBlocks, g->mpart, g->mv);
+    g_col_sum_parts<<<kMeanBlocks, kThreads, 0, s>>>(m, g->hc[R], g->mpart);
+    g_col_mean<<<1, H, 0, s>>>(m, kMeanBlocks, g->mpart, g->mcm);
     GCU(cudaGetLastError());
     return MC_OK;
 }
